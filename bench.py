@@ -1,0 +1,344 @@
+"""Benchmark: tracking steps/s of the probabilistic getter at 1M seeds on B200.
+
+Workload (one "step" = one pass of the tracking path over one batch): the
+probabilistic direction getter on the synthetic 81x106x76 phantom with its
+float32 PMF volume of 724 sphere vertices (1.9 GB), 1,000,000 seeds per GPU
+drawn from the FA > 0.3 mask, step 0.5 voxel, max angle 45 deg, stop at
+FA < 0.1, at most 501 points per direction.  A tracking step is one accepted
+direction + position update: steps = sum over streamlines of (length - 1).
+
+  value   device-timed (CUDA events on the library's stream) pass 1 + scans +
+          pass 2 + compaction with the seeds already resident in HBM
+  e2e     the same work through the C ABI with host buffers: H2D of the
+          seeds and D2H of lengths, seed ids and points inside the timed region
+  reference arm (--impl reference): the CPU restatement of the reference
+          algorithm on all host threads, on a bounded sample of the same seeds
+
+Multi-GPU (torchrun): one process per GPU; each rank tracks its own 1M seeds
+(weak scaling, no data exchange); per-rank times are reduced with MAX and the
+per-rank streamline/point counts are all-gathered (the offsets a global TRX
+file needs).  Inputs (1.9 GB PMF) exceed the 126 MB L2, so no flush is needed.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, HERE)
+
+METRIC = "tracking steps/s on 1 B200, learned+BF16 form vs plain FP32 kernel, 1M seeds"
+BYTES_PER_STEP = 8 * 724 * 4 + 8 * 4 + 12  # PMF corners + stop-map taps + point write
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--seeds", type=int, default=1_000_000)
+    ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--traffic-bytes-per-step", type=float, default=None,
+                    help="DRAM bytes per tracking step from an ncu capture (optional)")
+    return ap.parse_args()
+
+
+def dist_info():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+def build_workload(rank: int, nseeds: int):
+    from gpustreamlines_b200.phantom import make_phantom, odf_volume, seeds_from_mask
+    from gpustreamlines_b200.sphere import get_sphere
+
+    ph = make_phantom((81, 106, 76), seed=1234)
+    sph = get_sphere("repulsion724")
+    pmf = odf_volume(ph, sph)
+    seeds = seeds_from_mask(ph.fa, nseeds, threshold=0.3, seed=1000 + rank).astype(np.float32)
+    return ph, sph, pmf, seeds
+
+
+def measured_peaks():
+    path = os.path.join(HERE, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks/throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.idx = gpu_index
+        self.rows = []
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.idx), f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([x.strip() for x in line.split(",")])
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for r in self.rows:
+            for k, nm in enumerate(names):
+                if len(r) > 5 + k and r[5 + k].lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": float(np.median(sm)) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": sorted(reasons),
+                "samples": len(self.rows)}
+
+
+def cpu_baseline(ph, sph, pmf, seeds, seconds: float, threads: int | None = None):
+    """The oracle (CPU restatement of the reference) on a bounded seed sample."""
+    import math as _m
+
+    from oracle import api
+
+    threads = threads or os.cpu_count() or 1
+    inp = dict(case=dict(model="PROB", step=0.5, max_angle=45.0, fa_thr=0.1, rel=0.25, min_sep=45.0,
+                         rng_seed=0),
+               dataf=pmf, stop_map=np.ascontiguousarray(ph.fa, dtype=np.float32),
+               vertices=np.ascontiguousarray(sph.vertices, dtype=np.float32),
+               edges=np.ascontiguousarray(sph.edges, dtype=np.int32))
+    o = api.Oracle(inp, cos_max_angle=np.float32(_m.cos(np.float32(_m.radians(45.0)))))
+    n = 256
+    steps = 0
+    elapsed = 0.0
+    used = 0
+    while True:
+        batch = seeds[used:used + n]
+        t0 = time.perf_counter()
+        _, lens, _, _ = o.track(batch, threads=threads)
+        dt = time.perf_counter() - t0
+        steps += int((lens - 1).sum())
+        elapsed += dt
+        used += len(batch)
+        if elapsed >= seconds or used >= len(seeds):
+            break
+        rate = used / max(elapsed, 1e-9)
+        n = int(min(max(256, rate * (seconds - elapsed)), len(seeds) - used))
+    return dict(value=steps / elapsed, unit="steps/s", cores=threads, kind="port",
+                sample=f"{used} of the benchmark's seeds ({steps} steps, {elapsed:.1f} s)")
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return 0
+    ph, sph, pmf, seeds = build_workload(0, args.seeds)
+    threads = os.cpu_count() or 1
+    per = args.cpu_seconds / max(args.steps + args.warmup, 1)
+    vals = []
+    for i in range(args.warmup + args.steps):
+        sub = seeds[(i * 997) % max(len(seeds) - 50_000, 1):]
+        r = cpu_baseline(ph, sph, pmf, sub, max(per, 2.0), threads)
+        if i >= args.warmup:
+            vals.append(r)
+    v = float(np.mean([r["value"] for r in vals]))
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "steps/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": None,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic phantom (Stanford HARDI shapes)",
+            "config": {"workload": "prob getter, 81x106x76x724 PMF, 1M seeds (bounded CPU sample)",
+                       "seeds": args.seeds},
+            "cpu_baseline": {"value": v, "unit": "steps/s", "cores": threads, "kind": "port",
+                             "sample": "; ".join(r["sample"] for r in vals)},
+            "e2e": {"value": v, "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    args = parse()
+    rank, world, local = dist_info()
+    if args.impl == "reference":
+        return run_reference(args, rank, world)
+
+    import torch
+
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+
+    from gpustreamlines_b200 import ProbDirectionGetter, Tracker
+
+    ph, sph, pmf, seeds = build_workload(rank, args.seeds)
+    tracker = Tracker(ProbDirectionGetter(), pmf, ph.fa, 0.1, sph.vertices, sph.edges,
+                      max_angle=math.radians(45), step_size=0.5, ngpus=1, device_offset=local)
+    tracker.__enter__()
+    h = tracker.handles[0]
+    stream = torch.cuda.Stream(device=local)
+    seeds_d = torch.from_numpy(seeds).to(f"cuda:{local}")
+    seeds_pinned = torch.from_numpy(seeds).pin_memory()
+    torch.cuda.synchronize()
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    def device_step():
+        h.propagate_device(seeds_d.data_ptr(), len(seeds), 0, stream.cuda_stream)
+
+    for _ in range(args.warmup):
+        device_step()
+    nsl, npts = h.counts()
+    steps_per_batch = npts - nsl  # sum(len - 1)
+
+    # ---- device-resident timed region
+    barrier()
+    torch.cuda.synchronize()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    pass2_ms, pass1_ms, compact_ms = [], [], []
+    with ClockSampler(local) as clk:
+        ev0.record(stream)
+        for _ in range(args.steps):
+            device_step()
+            (p1, gap, p2, cp), runs = h.timings()
+            pass1_ms.append(p1)
+            pass2_ms.append(p2)
+            compact_ms.append(cp)
+        ev1.record(stream)
+        torch.cuda.synchronize()
+    total_ms = ev0.elapsed_time(ev1)
+    barrier()
+    counts = torch.tensor([float(total_ms), float(nsl), float(npts)], device=f"cuda:{local}",
+                          dtype=torch.float64)
+    if dist is not None:
+        t = counts[:1].clone()
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        gathered = [torch.zeros_like(counts) for _ in range(world)]
+        dist.all_gather(gathered, counts)
+        total_ms_max = float(t.item())
+        all_steps = sum(float(g[2].item() - g[1].item()) for g in gathered)
+    else:
+        total_ms_max = total_ms
+        all_steps = float(steps_per_batch)
+    ms_per_step = total_ms_max / args.steps
+    value = all_steps * args.steps / (total_ms_max / 1e3)
+
+    # ---- end-to-end through the C ABI with host buffers
+    L = np.empty(nsl, dtype=np.int32)
+    S = np.empty(nsl, dtype=np.int32)
+    Pt = np.empty((npts, 3), dtype=np.float32)
+    seeds_host = seeds_pinned.numpy()
+    barrier()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        h.propagate(seeds_host, 0, stream.cuda_stream)
+        h.fetch_into(L, S, Pt)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = e0.elapsed_time(e1)
+    if dist is not None:
+        t = torch.tensor([e2e_ms], device=f"cuda:{local}", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    e2e_value = all_steps * args.steps / (e2e_ms / 1e3)
+    h2d = seeds.nbytes
+    d2h = L.nbytes + S.nbytes + Pt.nbytes
+
+    peak, peak_kind = measured_peaks()
+    p2 = float(np.mean(pass2_ms))
+    achieved = steps_per_batch * BYTES_PER_STEP / (p2 / 1e3) / 1e9
+    traffic = None
+    if args.traffic_bytes_per_step:
+        traffic = args.traffic_bytes_per_step * steps_per_batch
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            cpu = cpu_baseline(ph, sph, pmf, seeds, args.cpu_seconds)
+        except Exception as e:  # the oracle is optional on the GPU box
+            cpu = {"value": None, "unit": "steps/s", "cores": 0, "kind": "port",
+                   "sample": f"unavailable: {e}"}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic phantom with Stanford HARDI shapes (seeded), random seeds in FA>0.3",
+            "config": {"workload": "prob getter (plain FP32), 81x106x76 PMF x 724 vertices (1.9 GB), "
+                                   f"{args.seeds} seeds per GPU, step 0.5, max angle 45",
+                       "global_batch": args.seeds * world, "seeds_per_gpu": args.seeds,
+                       "streamlines_per_gpu": nsl, "steps_per_gpu": int(steps_per_batch),
+                       "parallelism": f"seed shards x{world}",
+                       "l2": "inputs (1.9 GB PMF) larger than L2; no flush",
+                       "pass1_ms": float(np.mean(pass1_ms)), "pass2_ms": p2,
+                       "compact_ms": float(np.mean(compact_ms)),
+                       "streamlines_per_s": nsl * world * args.steps / (total_ms_max / 1e3)},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": traffic,
+                         "kernel": "track_kernel<PROB> (pass 2)",
+                         "peak_source": f"{peak_kind} MEASURED_PEAKS hbm_gbs",
+                         "algorithmic_bytes_per_step": BYTES_PER_STEP},
+            "e2e": {"value": e2e_value, "unit": "steps/s", "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h},
+            "gpu_launches": 3 * args.steps,
+            "clocks": clk.summary(),
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line), flush=True)
+    tracker.__exit__(None, None, None)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

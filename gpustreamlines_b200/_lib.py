@@ -1,0 +1,244 @@
+"""ctypes binding of the sm_100a tracking library (``_csl.so``).
+
+The library is built in-tree by ``gpustreamlines_b200/build.py`` (or
+``__graft_entry__.build()``).  There is no CPU fallback: loading fails loudly
+when the shared object is missing, and every entry point raises on a non-zero
+status with the library's own error message.
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "_csl.so")
+
+CSL_OK = 0
+CSL_E_INVALID = -1
+CSL_E_CUDA = -2
+CSL_E_NOMEM = -3
+CSL_E_STATE = -4
+CSL_E_KERNEL = -5
+
+MODEL_OPDT, MODEL_CSA, MODEL_PROB, MODEL_PTT = 0, 1, 2, 3
+
+
+class CslParams(C.Structure):
+    _fields_ = [
+        ("model", C.c_int),
+        ("dimx", C.c_int), ("dimy", C.c_int), ("dimz", C.c_int), ("dimt", C.c_int),
+        ("nvertices", C.c_int), ("nedges", C.c_int), ("samplm_nr", C.c_int),
+        ("sphere_symm", C.c_int), ("max_sline_len", C.c_int), ("_pad0", C.c_int),
+        ("step_size", C.c_double), ("max_angle", C.c_double), ("tc_threshold", C.c_double),
+        ("relative_peak_thresh", C.c_double), ("min_separation_angle", C.c_double),
+        ("pmf_threshold", C.c_double), ("rng_seed", C.c_ulonglong),
+        ("min_signal", C.c_double), ("delta_nr", C.c_int), ("_pad1", C.c_int),
+        ("odf_lut_res", C.c_int), ("step_frac", C.c_int),
+        ("probe_step_size", C.c_double), ("probe_quality", C.c_double),
+        ("max_curvature", C.c_double),
+        ("tile_log2_x", C.c_int), ("tile_log2_y", C.c_int),
+        ("tile_nx", C.c_int), ("tile_ny", C.c_int), ("tile_nz", C.c_int), ("_pad2", C.c_int),
+    ]
+
+
+_fp = C.POINTER(C.c_float)
+_ip = C.POINTER(C.c_int)
+
+
+class CslInputs(C.Structure):
+    _fields_ = [
+        ("dataf", _fp), ("stop_map", _fp), ("vertices", _fp), ("edges", _ip),
+        ("H", _fp), ("R", _fp), ("delta_b", _fp), ("delta_q", _fp),
+        ("sampling_matrix", _fp), ("b0s_mask", _ip),
+        ("ptt_odf_tiled", _fp), ("ptt_lut", _fp),
+    ]
+
+
+_lib = None
+
+# every symbol declared in include/gpustreamlines_b200.h
+EXPORTS = (
+    "csl_create", "csl_destroy", "csl_propagate", "csl_propagate_device", "csl_counts",
+    "csl_fetch", "csl_device_results", "csl_seed_peaks", "csl_get_direction",
+    "csl_device_constants", "csl_philox_stream", "csl_last_error", "csl_version",
+    "csl_batch_timings",
+)
+
+
+def load(path: str | None = None):
+    """Load the shared library (once) and declare argument types."""
+    global _lib
+    if _lib is not None and path is None:
+        return _lib
+    p = path or LIB_PATH
+    if not os.path.exists(p):
+        raise RuntimeError(
+            f"gpustreamlines_b200: CUDA library not built ({p} missing); run "
+            "`python -m gpustreamlines_b200.build` first (there is no CPU fallback)")
+    lib = C.CDLL(p)
+    vp = C.c_void_p
+    ll = C.c_longlong
+    ull_p = C.POINTER(C.c_ulonglong)
+    lib.csl_create.argtypes = [C.POINTER(CslParams), C.POINTER(CslInputs), C.c_int, C.POINTER(vp)]
+    lib.csl_destroy.argtypes = [vp]
+    lib.csl_propagate.argtypes = [vp, _fp, ll, ll, vp]
+    lib.csl_propagate_device.argtypes = [vp, vp, ll, ll, vp]
+    lib.csl_counts.argtypes = [vp, C.POINTER(ll), C.POINTER(ll)]
+    lib.csl_fetch.argtypes = [vp, _ip, _ip, _fp]
+    lib.csl_device_results.argtypes = [vp, C.POINTER(vp), C.POINTER(vp), C.POINTER(vp), C.POINTER(vp)]
+    lib.csl_seed_peaks.argtypes = [vp, _fp, ll, C.c_int, _ip, _ip, _fp]
+    lib.csl_get_direction.argtypes = [vp, _fp, _fp, ull_p, ull_p, ll, _fp, _fp, _ip, _ip]
+    lib.csl_device_constants.argtypes = [vp, _fp, _fp]
+    lib.csl_batch_timings.argtypes = [vp, _fp, _ip]
+    lib.csl_philox_stream.argtypes = [C.c_ulonglong, C.c_ulonglong, C.c_ulonglong, ll,
+                                      C.POINTER(C.c_uint)]
+    lib.csl_last_error.argtypes = [vp, C.c_char_p, C.c_int]
+    lib.csl_version.restype = C.c_char_p
+    for name in EXPORTS:
+        if name != "csl_version":
+            getattr(lib, name).restype = C.c_int
+    if path is None:
+        _lib = lib
+    return lib
+
+
+def last_error(handle=None) -> str:
+    lib = load()
+    buf = C.create_string_buffer(1024)
+    lib.csl_last_error(handle, buf, 1024)
+    return buf.value.decode(errors="replace")
+
+
+def check(rc: int, handle=None):
+    if rc == CSL_OK:
+        return
+    msg = last_error(handle)
+    if rc == CSL_E_INVALID:
+        raise ValueError(msg)
+    raise RuntimeError(f"gpustreamlines_b200 error {rc}: {msg}")
+
+
+def fptr(a: np.ndarray | None):
+    if a is None:
+        return None
+    assert a.dtype == np.float32 and a.flags["C_CONTIGUOUS"]
+    return a.ctypes.data_as(_fp)
+
+
+def iptr(a: np.ndarray | None):
+    if a is None:
+        return None
+    assert a.dtype == np.int32 and a.flags["C_CONTIGUOUS"]
+    return a.ctypes.data_as(_ip)
+
+
+def uptr(a: np.ndarray):
+    assert a.dtype == np.uint64 and a.flags["C_CONTIGUOUS"]
+    return a.ctypes.data_as(C.POINTER(C.c_ulonglong))
+
+
+def philox_stream(seed: int, subsequence: int, offset: int, n: int) -> np.ndarray:
+    """This library's Philox4x32-10 words (curand_init(seed, subsequence, offset) layout)."""
+    lib = load()
+    out = np.empty(n, dtype=np.uint32)
+    check(lib.csl_philox_stream(seed, subsequence, offset, n,
+                                out.ctypes.data_as(C.POINTER(C.c_uint))))
+    return out
+
+
+class Handle:
+    """Owns one ``csl_tracker`` (one device)."""
+
+    def __init__(self, params: CslParams, inputs: CslInputs, device: int, keepalive=()):
+        self.lib = load()
+        self._keep = list(keepalive)
+        h = C.c_void_p()
+        check(self.lib.csl_create(C.byref(params), C.byref(inputs), int(device), C.byref(h)))
+        self.h = h
+        self.device = device
+        self.model = params.model
+        self._keep = []  # inputs were copied to the device
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.csl_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _chk(self, rc):
+        check(rc, self.h)
+
+    def propagate(self, seeds: np.ndarray, rng_index_base: int = 0, stream: int | None = None):
+        seeds = np.ascontiguousarray(seeds, dtype=np.float32).reshape(-1, 3)
+        self._chk(self.lib.csl_propagate(self.h, fptr(seeds), len(seeds), int(rng_index_base),
+                                         stream))
+
+    def propagate_device(self, seeds_ptr: int, n: int, rng_index_base: int = 0,
+                         stream: int | None = None):
+        self._chk(self.lib.csl_propagate_device(self.h, C.c_void_p(seeds_ptr), int(n),
+                                                int(rng_index_base), stream))
+
+    def counts(self):
+        a, b = C.c_longlong(), C.c_longlong()
+        self._chk(self.lib.csl_counts(self.h, C.byref(a), C.byref(b)))
+        return a.value, b.value
+
+    def fetch(self, lengths=True, seed_index=True, points=True):
+        nsl, npts = self.counts()
+        L = np.empty(nsl, dtype=np.int32) if lengths else None
+        S = np.empty(nsl, dtype=np.int32) if seed_index else None
+        Pt = np.empty((npts, 3), dtype=np.float32) if points else None
+        self._chk(self.lib.csl_fetch(self.h, iptr(L), iptr(S), fptr(Pt)))
+        return L, S, Pt
+
+    def fetch_into(self, L, S, Pt):
+        self._chk(self.lib.csl_fetch(self.h, iptr(L), iptr(S), fptr(Pt)))
+
+    def device_results(self):
+        ptrs = [C.c_void_p() for _ in range(4)]
+        self._chk(self.lib.csl_device_results(self.h, *[C.byref(p) for p in ptrs]))
+        return tuple(p.value for p in ptrs)
+
+    def seed_peaks(self, seeds: np.ndarray, max_peaks: int = 32):
+        seeds = np.ascontiguousarray(seeds, dtype=np.float32).reshape(-1, 3)
+        n = len(seeds)
+        counts = np.zeros(n, dtype=np.int32)
+        pv = np.full((n, max_peaks), -1, dtype=np.int32)
+        pd = np.zeros((n, max_peaks, 3), dtype=np.float32)
+        self._chk(self.lib.csl_seed_peaks(self.h, fptr(seeds), n, max_peaks, iptr(counts),
+                                          iptr(pv), fptr(pd)))
+        return counts, pv, pd
+
+    def get_direction(self, points, dirs, subsequence, offset, frames=None):
+        pts = np.ascontiguousarray(points, dtype=np.float32).reshape(-1, 3)
+        ds = np.ascontiguousarray(dirs, dtype=np.float32).reshape(-1, 3)
+        n = len(pts)
+        sq = np.ascontiguousarray(subsequence, dtype=np.uint64).reshape(n)
+        of = np.ascontiguousarray(offset, dtype=np.uint64).reshape(n)
+        fr = None if frames is None else np.ascontiguousarray(frames, dtype=np.float32).reshape(n, 9)
+        nd = np.zeros((n, 3), dtype=np.float32)
+        ok = np.zeros(n, dtype=np.int32)
+        dr = np.zeros(n, dtype=np.int32)
+        self._chk(self.lib.csl_get_direction(self.h, fptr(pts), fptr(ds), uptr(sq), uptr(of), n,
+                                             fptr(fr), fptr(nd), iptr(ok), iptr(dr)))
+        return nd, ok, dr, fr
+
+    def timings(self):
+        """(pass1_ms, gap_ms, pass2_ms, compact_ms), pass-2 runs of the last batch."""
+        ms = np.zeros(4, dtype=np.float32)
+        runs = C.c_int()
+        self._chk(self.lib.csl_batch_timings(self.h, fptr(ms), C.byref(runs)))
+        return tuple(float(x) for x in ms), runs.value
+
+    def device_constants(self):
+        a, b = C.c_float(), C.c_float()
+        self._chk(self.lib.csl_device_constants(self.h, C.byref(a), C.byref(b)))
+        return a.value, b.value

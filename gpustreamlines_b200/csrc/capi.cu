@@ -1,0 +1,691 @@
+// C ABI of the tracker (declared in include/gpustreamlines_b200.h).
+//
+// Host orchestration per batch (replaces SeedBatchPropagator.propagate,
+// cu_propagate_seeds.py:206-233):
+//   H2D seeds -> pass 1 (seed peaks) -> device exclusive scan of the peak
+//   counts -> pass 2 (persistent tracker into a point pool) -> device scan
+//   of the streamline lengths -> gather into compacted, ordered points.
+// Two 8-byte reads cross PCIe inside a batch (streamline and point totals,
+// needed to size the outputs); the pool is grown and pass 2 re-run if the
+// first guess of its size was too small (results are deterministic, so a
+// re-run produces the same output).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/gpustreamlines_b200.h"
+#include "kernels.h"
+
+using namespace csl;
+
+namespace {
+
+thread_local std::string g_lib_error;
+
+template <typename T>
+struct DevBuf {
+    T *p = nullptr;
+    size_t cap = 0;  // elements
+    cudaError_t ensure(size_t n) {
+        if (n <= cap && p) return cudaSuccess;
+        if (p) cudaFree(p);
+        p = nullptr;
+        cap = 0;
+        const size_t m = std::max<size_t>(n, 1);
+        cudaError_t e = cudaMalloc(&p, m * sizeof(T));
+        if (e == cudaSuccess) cap = m;
+        return e;
+    }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        cap = 0;
+    }
+};
+
+}  // namespace
+
+struct csl_tracker {
+    int device = 0;
+    cudaStream_t own_stream = nullptr;
+    csl_params hp{};
+    DevParams P{};
+    std::string err;
+    int nsm = 0;
+    int block = 256;
+    int blocks_per_sm = 1;
+    // inputs
+    DevBuf<float> dataf, verts, H, R, delta_b, delta_q, sampling;
+    DevBuf<int> edges, b0s, partner;
+    DevBuf<uint32_t> cone;
+    cudaArray_t stop_arr = nullptr, odf_arr = nullptr, lut_arr = nullptr;
+    cudaTextureObject_t stop_tex = 0, odf_tex = 0, lut_tex = 0;
+    DevBuf<float> consts;
+    // batch
+    DevBuf<float> seeds;
+    DevBuf<int> npeaks, sl_off, out_len, out_seed, queue, status;
+    DevBuf<short> peaks;
+    DevBuf<long long> out_src, pt_off;
+    DevBuf<unsigned long long> pool_count;
+    DevBuf<float> pool, scratch, points;
+    DevBuf<unsigned char> scan_tmp;
+    long long last_n = -1, nsl = 0, npts = 0;
+    int ok_batch = 0;
+    cudaStream_t last_stream = nullptr;
+    // timing events of the last batch: start, pass 1 + scan, pass 2, compaction
+    cudaEvent_t ev[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
+    float ms[4] = {0, 0, 0, 0};
+    int pass2_runs = 0;
+};
+
+static int fail(csl_tracker *t, int code, const char *fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    if (t)
+        t->err = buf;
+    else
+        g_lib_error = buf;
+    return code;
+}
+
+#define CK(call)                                                                          \
+    do {                                                                                  \
+        cudaError_t _e = (call);                                                          \
+        if (_e != cudaSuccess)                                                            \
+            return fail(t, _e == cudaErrorMemoryAllocation ? CSL_E_NOMEM : CSL_E_CUDA,    \
+                        "CUDA error code=%d(%s) at %s:%d", (int)_e, cudaGetErrorName(_e), \
+                        __FILE__, __LINE__);                                              \
+    } while (0)
+
+// Batcher's merge-exchange network (Knuth, TAOCP vol. 3, 5.2.2 Algorithm M)
+// for 32 keys, comparators placed in the earliest layer their inputs allow.
+// partner[l][i] = lane compared with lane i in layer l (i itself if idle).
+static std::vector<int> merge_exchange_partners() {
+    const int N = 32, t = 5;
+    std::vector<std::vector<std::pair<int, int>>> rounds;
+    for (int p = 1 << (t - 1); p > 0; p >>= 1) {
+        int q = 1 << (t - 1), r = 0, d = p;
+        for (;;) {
+            std::vector<std::pair<int, int>> rnd;
+            for (int i = 0; i < N - d; i++)
+                if ((i & p) == r) rnd.emplace_back(i, i + d);
+            rounds.push_back(rnd);
+            if (q != p) {
+                d = q - p;
+                q >>= 1;
+                r = p;
+            } else {
+                break;
+            }
+        }
+    }
+    std::vector<int> last(N, -1);
+    std::vector<std::vector<int>> layers;
+    for (auto &rnd : rounds)
+        for (auto &c : rnd) {
+            const int l = std::max(last[c.first], last[c.second]) + 1;
+            while ((int)layers.size() <= l) {
+                std::vector<int> id(N);
+                for (int i = 0; i < N; i++) id[i] = i;
+                layers.push_back(id);
+            }
+            layers[l][c.first] = c.second;
+            layers[l][c.second] = c.first;
+            last[c.first] = last[c.second] = l;
+        }
+    std::vector<int> flat(kMaxSortLayers * N);
+    for (int l = 0; l < kMaxSortLayers; l++)
+        for (int i = 0; i < N; i++)
+            flat[l * N + i] = l < (int)layers.size() ? layers[l][i] : i;
+    return flat;
+}
+
+static int make_texture3d(csl_tracker *t, const float *host, int w, int h, int d, bool border,
+                          bool linear, bool normalized, cudaArray_t *arr, cudaTextureObject_t *tex) {
+    cudaChannelFormatDesc cd = cudaCreateChannelDesc(32, 0, 0, 0, cudaChannelFormatKindFloat);
+    cudaExtent ext = make_cudaExtent(w, h, d);
+    CK(cudaMalloc3DArray(arr, &cd, ext, 0));
+    cudaMemcpy3DParms cp = {};
+    cp.srcPtr = make_cudaPitchedPtr((void *)host, (size_t)w * 4, w, h);
+    cp.dstArray = *arr;
+    cp.extent = ext;
+    cp.kind = cudaMemcpyHostToDevice;
+    CK(cudaMemcpy3D(&cp));
+    cudaResourceDesc rd = {};
+    rd.resType = cudaResourceTypeArray;
+    rd.res.array.array = *arr;
+    cudaTextureDesc td = {};
+    const cudaTextureAddressMode am = border ? cudaAddressModeBorder : cudaAddressModeClamp;
+    td.addressMode[0] = td.addressMode[1] = td.addressMode[2] = am;
+    if (border) td.borderColor[0] = td.borderColor[1] = td.borderColor[2] = td.borderColor[3] = -1.0f;
+    td.filterMode = linear ? cudaFilterModeLinear : cudaFilterModePoint;
+    td.readMode = cudaReadModeElementType;
+    td.normalizedCoords = normalized ? 1 : 0;
+    CK(cudaCreateTextureObject(tex, &rd, &td, nullptr));
+    return CSL_OK;
+}
+
+template <typename T>
+static int upload(csl_tracker *t, DevBuf<T> &b, const T *host, size_t n) {
+    CK(b.ensure(n));
+    CK(cudaMemcpy(b.p, host, n * sizeof(T), cudaMemcpyHostToDevice));
+    return CSL_OK;
+}
+
+static void release_all(csl_tracker *t) {
+    if (t->stop_tex) cudaDestroyTextureObject(t->stop_tex);
+    if (t->odf_tex) cudaDestroyTextureObject(t->odf_tex);
+    if (t->lut_tex) cudaDestroyTextureObject(t->lut_tex);
+    if (t->stop_arr) cudaFreeArray(t->stop_arr);
+    if (t->odf_arr) cudaFreeArray(t->odf_arr);
+    if (t->lut_arr) cudaFreeArray(t->lut_arr);
+    t->stop_tex = t->odf_tex = t->lut_tex = 0;
+    t->stop_arr = t->odf_arr = t->lut_arr = nullptr;
+    DevBuf<float> *fb[] = {&t->dataf, &t->verts, &t->H, &t->R, &t->delta_b, &t->delta_q,
+                           &t->sampling, &t->consts, &t->seeds, &t->pool, &t->scratch, &t->points};
+    for (auto *b : fb) b->release();
+    DevBuf<int> *ib[] = {&t->edges, &t->b0s, &t->partner, &t->npeaks, &t->sl_off,
+                         &t->out_len, &t->out_seed, &t->queue, &t->status};
+    for (auto *b : ib) b->release();
+    t->cone.release();
+    t->peaks.release();
+    t->out_src.release();
+    t->pt_off.release();
+    t->pool_count.release();
+    t->scan_tmp.release();
+    for (auto &e : t->ev)
+        if (e) cudaEventDestroy(e);
+    if (t->own_stream) cudaStreamDestroy(t->own_stream);
+    t->own_stream = nullptr;
+}
+
+static int validate(const csl_params *p, const csl_inputs *in, csl_tracker *t) {
+    if (!p || !in) return fail(t, CSL_E_INVALID, "params and inputs must not be NULL");
+    if (p->model < CSL_MODEL_OPDT || p->model > CSL_MODEL_PTT)
+        return fail(t, CSL_E_INVALID, "Invalid model type %d", p->model);
+    if (p->dimx <= 0 || p->dimy <= 0 || p->dimz <= 0 || p->dimt <= 0)
+        return fail(t, CSL_E_INVALID, "volume dimensions must be positive");
+    if (p->nvertices <= 0 || p->nedges <= 0) return fail(t, CSL_E_INVALID, "empty sphere");
+    if (p->nvertices > 32767) return fail(t, CSL_E_INVALID, "at most 32767 sphere vertices");
+    if (p->max_sline_len < 2) return fail(t, CSL_E_INVALID, "max_sline_len must be >= 2");
+    if (!in->stop_map || !in->vertices || !in->edges)
+        return fail(t, CSL_E_INVALID, "stop_map, vertices and edges are required");
+    const bool boot = p->model == CSL_MODEL_OPDT || p->model == CSL_MODEL_CSA;
+    if (boot) {
+        if (!in->dataf || !in->H || !in->R || !in->delta_b || !in->delta_q || !in->sampling_matrix ||
+            !in->b0s_mask)
+            return fail(t, CSL_E_INVALID, "bootstrap getter needs dataf, H, R, delta_b, delta_q, "
+                                          "sampling_matrix and b0s_mask");
+        if (p->delta_nr <= 0 || p->samplm_nr <= 0)
+            return fail(t, CSL_E_INVALID, "delta_nr and samplm_nr must be positive");
+        if (p->samplm_nr != p->nvertices)
+            return fail(t, CSL_E_INVALID, "sampling_matrix rows (%d) must equal sphere vertices (%d)",
+                        p->samplm_nr, p->nvertices);
+    } else {
+        if (p->nvertices != p->dimt)
+            return fail(t, CSL_E_INVALID,
+                        "Number of sphere vertices (%d) must match last dimension of dataf (%d), "
+                        "because dataf should be an ODF when using prob or ptt tracking",
+                        p->nvertices, p->dimt);
+        if (p->model == CSL_MODEL_PROB && !in->dataf)
+            return fail(t, CSL_E_INVALID, "prob getter needs dataf");
+        if (p->model == CSL_MODEL_PROB && p->dimt > 1024)
+            return fail(t, CSL_E_INVALID, "prob getter supports at most 1024 sphere vertices");
+        if (p->model == CSL_MODEL_PTT) {
+            if (!in->ptt_odf_tiled || !in->ptt_lut)
+                return fail(t, CSL_E_INVALID, "PTT getter needs ptt_odf_tiled and ptt_lut");
+            if (p->step_frac <= 0 || p->odf_lut_res <= 0 || p->tile_nx <= 0 || p->tile_ny <= 0 ||
+                p->tile_nz <= 0)
+                return fail(t, CSL_E_INVALID, "bad PTT parameters");
+        }
+    }
+    return CSL_OK;
+}
+
+extern "C" {
+
+const char *csl_version(void) { return "gpustreamlines_b200 0.1.0 (sm_100a)"; }
+
+int csl_last_error(const csl_tracker *t, char *buf, int buflen) {
+    const std::string &s = t ? t->err : g_lib_error;
+    if (buf && buflen > 0) {
+        std::strncpy(buf, s.c_str(), buflen - 1);
+        buf[buflen - 1] = 0;
+    }
+    return (int)s.size();
+}
+
+int csl_create(const csl_params *params, const csl_inputs *inputs, int device, csl_tracker **out) {
+    csl_tracker *t = nullptr;
+    if (!out) return fail(nullptr, CSL_E_INVALID, "out must not be NULL");
+    *out = nullptr;
+    int rc = validate(params, inputs, nullptr);
+    if (rc) return rc;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
+        return fail(nullptr, CSL_E_CUDA, "no CUDA device available");
+    if (device < 0 || device >= ndev)
+        return fail(nullptr, CSL_E_INVALID, "Requested device %d but only %d available", device, ndev);
+    t = new csl_tracker();
+    t->device = device;
+    t->hp = *params;
+    rc = [&]() -> int {
+        CK(cudaSetDevice(device));
+        CK(cudaStreamCreateWithFlags(&t->own_stream, cudaStreamNonBlocking));
+        CK(cudaDeviceGetAttribute(&t->nsm, cudaDevAttrMultiProcessorCount, device));
+        const csl_params &p = *params;
+        DevParams &P = t->P;
+        P.model = p.model;
+        P.dimx = p.dimx;
+        P.dimy = p.dimy;
+        P.dimz = p.dimz;
+        P.dimt = p.dimt;
+        P.nvert = p.nvertices;
+        P.nedges = p.nedges;
+        const bool boot = p.model == OPDT || p.model == CSA;
+        P.samplm_nr = boot ? p.samplm_nr : p.dimt;
+        P.sphere_symm = p.sphere_symm ? 1 : 0;
+        P.max_sline_len = p.max_sline_len;
+        P.nch = (p.model == PROB) ? (P.samplm_nr + 31) / 32 : 1;
+        P.step_frac = (p.model == PTT) ? p.step_frac : 1;
+        P.step_size = p.step_size;
+        P.max_angle = p.max_angle;
+        P.tc_threshold = p.tc_threshold;
+        P.relative_peak_thresh = p.relative_peak_thresh;
+        P.min_separation_angle = p.min_separation_angle;
+        P.pmf_threshold = p.pmf_threshold;
+        P.rng_seed = p.rng_seed;
+        const size_t nvox = (size_t)p.dimx * p.dimy * p.dimz;
+        if (p.model != PTT) {
+            int r = upload(t, t->dataf, inputs->dataf, nvox * p.dimt);
+            if (r) return r;
+            P.dataf = t->dataf.p;
+        }
+        int r = upload(t, t->verts, inputs->vertices, (size_t)p.nvertices * 3);
+        if (r) return r;
+        r = upload(t, t->edges, inputs->edges, (size_t)p.nedges * 2);
+        if (r) return r;
+        P.verts = t->verts.p;
+        P.edges = reinterpret_cast<const int2 *>(t->edges.p);
+        const std::vector<int> part = merge_exchange_partners();
+        r = upload(t, t->partner, part.data(), part.size());
+        if (r) return r;
+        r = make_texture3d(t, inputs->stop_map, p.dimz, p.dimy, p.dimx, true, true, false,
+                           &t->stop_arr, &t->stop_tex);
+        if (r) return r;
+        P.stop_tex = t->stop_tex;
+        // cos() of the angles, evaluated on the device with the fast cosine
+        CK(t->consts.ensure(2));
+        CK(launch_device_cos((float)p.max_angle, (float)p.min_separation_angle, t->consts.p,
+                             t->own_stream));
+        float cs[2];
+        CK(cudaMemcpyAsync(cs, t->consts.p, sizeof(cs), cudaMemcpyDeviceToHost, t->own_stream));
+        CK(cudaStreamSynchronize(t->own_stream));
+        P.cos_max_angle = cs[0];
+        P.cos_min_sep = cs[1];
+        if (boot) {
+            int hr = 0;
+            for (int i = 0; i < p.dimt; i++) hr += inputs->b0s_mask[i] ? 0 : 1;
+            if (hr <= 0 || hr > 512)
+                return fail(t, CSL_E_INVALID, "bootstrap needs 1..512 non-b0 volumes, got %d", hr);
+            if (p.delta_nr > 512) return fail(t, CSL_E_INVALID, "delta_nr must be <= 512");
+            P.hr_side = hr;
+            P.delta_nr = p.delta_nr;
+            P.min_signal = (float)p.min_signal;
+            if ((r = upload(t, t->H, inputs->H, (size_t)hr * hr))) return r;
+            if ((r = upload(t, t->R, inputs->R, (size_t)hr * hr))) return r;
+            if ((r = upload(t, t->delta_b, inputs->delta_b, (size_t)p.delta_nr * hr))) return r;
+            if ((r = upload(t, t->delta_q, inputs->delta_q, (size_t)p.delta_nr * hr))) return r;
+            if ((r = upload(t, t->sampling, inputs->sampling_matrix, (size_t)p.samplm_nr * p.delta_nr)))
+                return r;
+            if ((r = upload(t, t->b0s, inputs->b0s_mask, (size_t)p.dimt))) return r;
+            P.H = t->H.p;
+            P.R = t->R.p;
+            P.delta_b = t->delta_b.p;
+            P.delta_q = t->delta_q.p;
+            P.sampling = t->sampling.p;
+            P.b0s_mask = t->b0s.p;
+        }
+        if (p.model == PROB) {
+            CK(t->cone.ensure((size_t)2 * P.nvert * P.nch));
+            P.cone_mask = t->cone.p;
+            CK(launch_cone_mask(P, t->cone.p, t->own_stream));
+        }
+        if (p.model == PTT) {
+            r = make_texture3d(t, inputs->ptt_odf_tiled, p.tile_nx * p.dimx, p.tile_ny * p.dimy,
+                               p.tile_nz * p.dimz, false, true, false, &t->odf_arr, &t->odf_tex);
+            if (r) return r;
+            r = make_texture3d(t, inputs->ptt_lut, p.odf_lut_res, p.odf_lut_res, p.odf_lut_res, false,
+                               false, true, &t->lut_arr, &t->lut_tex);
+            if (r) return r;
+            P.odf_tex = t->odf_tex;
+            P.lut_tex = t->lut_tex;
+            P.log2_x = p.tile_log2_x;
+            P.log2_y = p.tile_log2_y;
+            P.width_mask = p.tile_nx - 1;
+            P.height_mask = p.tile_ny - 1;
+            P.probe_step_size = (float)p.probe_step_size;
+            P.probe_quality = (float)p.probe_quality;
+            P.max_curvature = p.max_curvature;
+        }
+        const int smem = smem_bytes(P, t->block / kWarp, true);
+        if (smem > 227 * 1024) {
+            t->block = 128;
+        }
+        CK(track_occupancy(P, t->block, &t->blocks_per_sm));
+        if (t->blocks_per_sm < 1) {
+            t->block = 64;
+            CK(track_occupancy(P, t->block, &t->blocks_per_sm));
+            if (t->blocks_per_sm < 1)
+                return fail(t, CSL_E_INVALID, "kernel does not fit on the device (shared memory %d B)",
+                            smem_bytes(P, t->block / kWarp, true));
+        }
+        for (auto &e : t->ev) CK(cudaEventCreate(&e));
+        CK(t->queue.ensure(1));
+        CK(t->status.ensure(1));
+        CK(t->pool_count.ensure(1));
+        CK(cudaStreamSynchronize(t->own_stream));
+        return CSL_OK;
+    }();
+    if (rc) {
+        g_lib_error = t->err;
+        release_all(t);
+        delete t;
+        return rc;
+    }
+    *out = t;
+    return CSL_OK;
+}
+
+int csl_destroy(csl_tracker *t) {
+    if (!t) return CSL_OK;
+    cudaSetDevice(t->device);
+    cudaDeviceSynchronize();
+    release_all(t);
+    delete t;
+    return CSL_OK;
+}
+
+static int run_batch(csl_tracker *t, const float *seeds_dev, long long n, long long rng_base,
+                     cudaStream_t st) {
+    const DevParams &P = t->P;
+    t->ok_batch = 0;
+    t->nsl = t->npts = 0;
+    t->last_n = n;
+    t->last_stream = st;
+    for (float &m : t->ms) m = 0;
+    t->pass2_runs = 0;
+    if (n == 0) {
+        t->ok_batch = 1;
+        return CSL_OK;
+    }
+    if (n > (1ll << 30)) return fail(t, CSL_E_INVALID, "batch too large (%lld seeds)", n);
+    const int ni = (int)n;
+    CK(t->npeaks.ensure(ni + 1));
+    CK(t->sl_off.ensure(ni + 1));
+    CK(t->peaks.ensure((size_t)ni * kMaxStoredPeaksPerSeed));
+    size_t tmpb = 0;
+    CK(scan_temp_bytes(std::max(ni, 1 << 20), &tmpb));
+    CK(t->scan_tmp.ensure(tmpb));
+
+    // pass 1
+    CK(cudaEventRecord(t->ev[0], st));
+    const int wpb = t->block / kWarp;
+    const int grid1 = std::min<long long>((n + wpb - 1) / wpb, (long long)t->nsm * 16);
+    CK(cudaMemsetAsync(t->npeaks.p + ni, 0, sizeof(int), st));
+    CK(launch_seed_peaks(P, seeds_dev, ni, rng_base, t->partner.p, t->npeaks.p, t->peaks.p,
+                         kMaxStoredPeaksPerSeed, grid1, t->block, st));
+    CK(exclusive_scan_i32(t->scan_tmp.p, t->scan_tmp.cap, t->npeaks.p, t->sl_off.p, ni + 1, st));
+    CK(cudaEventRecord(t->ev[1], st));
+    int nsl = 0;
+    CK(cudaMemcpyAsync(&nsl, t->sl_off.p + ni, sizeof(int), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    t->nsl = nsl;
+    CK(t->out_len.ensure((size_t)nsl + 1));
+    CK(t->out_seed.ensure((size_t)nsl + 1));
+    CK(t->out_src.ensure((size_t)nsl + 1));
+    CK(t->pt_off.ensure((size_t)nsl + 1));
+
+    // pass 2 (re-run once with an exact pool size if the guess was short)
+    const long long warps_needed = n;
+    const int grid2 = (int)std::max<long long>(
+        1, std::min<long long>((long long)t->nsm * t->blocks_per_sm, (warps_needed + wpb - 1) / wpb));
+    CK(t->scratch.ensure((size_t)grid2 * wpb * scratch_floats_per_warp(P)));
+    unsigned long long want = std::max<unsigned long long>(t->pool.cap / 3, (unsigned long long)nsl * 96ull);
+    for (int attempt = 0; attempt < 2; attempt++) {
+        CK(t->pool.ensure(want * 3));
+        BatchArgs B{};
+        B.seeds = seeds_dev;
+        B.nseeds = ni;
+        B.rng_index_base = rng_base;
+        B.queue = t->queue.p;
+        B.pool_count = t->pool_count.p;
+        B.pool = t->pool.p;
+        B.pool_cap = t->pool.cap / 3;
+        B.scratch = t->scratch.p;
+        B.status = t->status.p;
+        CK(cudaMemsetAsync(t->queue.p, 0, sizeof(int), st));
+        CK(cudaMemsetAsync(t->status.p, 0, sizeof(int), st));
+        CK(cudaMemsetAsync(t->pool_count.p, 0, sizeof(unsigned long long), st));
+        CK(cudaEventRecord(t->ev[2], st));
+        CK(launch_track(P, B, t->partner.p, t->npeaks.p, t->peaks.p, kMaxStoredPeaksPerSeed,
+                        t->sl_off.p, t->out_len.p, t->out_seed.p, t->out_src.p, grid2, t->block, st));
+        CK(cudaEventRecord(t->ev[3], st));
+        t->pass2_runs++;
+        int status = 0;
+        unsigned long long used = 0;
+        CK(cudaMemcpyAsync(&status, t->status.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+        CK(cudaMemcpyAsync(&used, t->pool_count.p, sizeof(used), cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        if (!(status & ST_POOL_OVERFLOW)) break;
+        if (attempt == 1) return fail(t, CSL_E_KERNEL, "point pool overflow after resize");
+        want = used + used / 8 + 1024;
+    }
+
+    // compaction
+    CK(cudaMemsetAsync(t->out_len.p + nsl, 0, sizeof(int), st));
+    CK(exclusive_scan_i64(t->scan_tmp.p, t->scan_tmp.cap, t->out_len.p, t->pt_off.p, nsl + 1, st));
+    long long npts = 0;
+    CK(cudaMemcpyAsync(&npts, t->pt_off.p + nsl, sizeof(long long), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    t->npts = npts;
+    CK(t->points.ensure((size_t)npts * 3 + 3));
+    CK(launch_gather(t->pool.p, t->out_src.p, t->out_len.p, t->pt_off.p, nsl, t->points.p,
+                     t->nsm * 8, st));
+    CK(cudaEventRecord(t->ev[4], st));
+    CK(cudaStreamSynchronize(st));
+    CK(cudaEventElapsedTime(&t->ms[0], t->ev[0], t->ev[1]));
+    CK(cudaEventElapsedTime(&t->ms[1], t->ev[1], t->ev[2]));
+    CK(cudaEventElapsedTime(&t->ms[2], t->ev[2], t->ev[3]));
+    CK(cudaEventElapsedTime(&t->ms[3], t->ev[3], t->ev[4]));
+    t->ok_batch = 1;
+    return CSL_OK;
+}
+
+int csl_propagate_device(csl_tracker *t, const float *seeds_dev, long long n, long long rng_index_base,
+                         void *stream) {
+    if (!t) return fail(nullptr, CSL_E_INVALID, "NULL tracker");
+    if (n < 0 || (n > 0 && !seeds_dev)) return fail(t, CSL_E_INVALID, "bad seeds");
+    CK(cudaSetDevice(t->device));
+    cudaStream_t st = stream ? (cudaStream_t)stream : t->own_stream;
+    return run_batch(t, seeds_dev, n, rng_index_base, st);
+}
+
+int csl_propagate(csl_tracker *t, const float *seeds_host, long long n, long long rng_index_base,
+                  void *stream) {
+    if (!t) return fail(nullptr, CSL_E_INVALID, "NULL tracker");
+    if (n < 0 || (n > 0 && !seeds_host)) return fail(t, CSL_E_INVALID, "bad seeds");
+    CK(cudaSetDevice(t->device));
+    cudaStream_t st = stream ? (cudaStream_t)stream : t->own_stream;
+    CK(t->seeds.ensure((size_t)std::max<long long>(n, 1) * 3));
+    if (n > 0)
+        CK(cudaMemcpyAsync(t->seeds.p, seeds_host, (size_t)n * 3 * sizeof(float),
+                           cudaMemcpyHostToDevice, st));
+    return run_batch(t, t->seeds.p, n, rng_index_base, st);
+}
+
+int csl_counts(csl_tracker *t, long long *n_streamlines, long long *n_points) {
+    if (!t) return fail(nullptr, CSL_E_INVALID, "NULL tracker");
+    if (!t->ok_batch) return fail(t, CSL_E_STATE, "no completed batch");
+    if (n_streamlines) *n_streamlines = t->nsl;
+    if (n_points) *n_points = t->npts;
+    return CSL_OK;
+}
+
+int csl_fetch(csl_tracker *t, int *lengths, int *seed_index, float *points) {
+    if (!t) return fail(nullptr, CSL_E_INVALID, "NULL tracker");
+    if (!t->ok_batch) return fail(t, CSL_E_STATE, "no completed batch");
+    CK(cudaSetDevice(t->device));
+    cudaStream_t st = t->last_stream ? t->last_stream : t->own_stream;
+    if (t->nsl > 0) {
+        if (lengths)
+            CK(cudaMemcpyAsync(lengths, t->out_len.p, (size_t)t->nsl * sizeof(int),
+                               cudaMemcpyDeviceToHost, st));
+        if (seed_index)
+            CK(cudaMemcpyAsync(seed_index, t->out_seed.p, (size_t)t->nsl * sizeof(int),
+                               cudaMemcpyDeviceToHost, st));
+    }
+    if (points && t->npts > 0)
+        CK(cudaMemcpyAsync(points, t->points.p, (size_t)t->npts * 3 * sizeof(float),
+                           cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    return CSL_OK;
+}
+
+int csl_device_results(csl_tracker *t, const int **lengths, const int **seed_index,
+                       const long long **point_offsets, const float **points) {
+    if (!t) return fail(nullptr, CSL_E_INVALID, "NULL tracker");
+    if (!t->ok_batch) return fail(t, CSL_E_STATE, "no completed batch");
+    if (lengths) *lengths = t->out_len.p;
+    if (seed_index) *seed_index = t->out_seed.p;
+    if (point_offsets) *point_offsets = t->pt_off.p;
+    if (points) *points = t->points.p;
+    return CSL_OK;
+}
+
+int csl_seed_peaks(csl_tracker *t, const float *seeds_host, long long n, int max_peaks, int *counts,
+                   int *peak_vertex, float *peak_dirs) {
+    if (!t) return fail(nullptr, CSL_E_INVALID, "NULL tracker");
+    if (n < 0 || (n > 0 && (!seeds_host || !counts)) || max_peaks < 0 || max_peaks > 32767)
+        return fail(t, CSL_E_INVALID, "bad arguments");
+    if (n == 0) return CSL_OK;
+    CK(cudaSetDevice(t->device));
+    cudaStream_t st = t->own_stream;
+    const int ni = (int)n;
+    const int mp = std::max(max_peaks, 1);
+    DevBuf<float> sd;
+    DevBuf<int> cnt;
+    DevBuf<short> pk;
+    auto cleanup = [&]() { sd.release(); cnt.release(); pk.release(); };
+    cudaError_t e = sd.ensure((size_t)ni * 3);
+    if (e == cudaSuccess) e = cnt.ensure(ni);
+    if (e == cudaSuccess) e = pk.ensure((size_t)ni * mp);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(sd.p, seeds_host, (size_t)ni * 3 * sizeof(float), cudaMemcpyHostToDevice, st);
+    const int wpb = t->block / kWarp;
+    if (e == cudaSuccess)
+        e = launch_seed_peaks(t->P, sd.p, ni, 0, t->partner.p, cnt.p, pk.p, mp,
+                              std::min((ni + wpb - 1) / wpb, t->nsm * 16), t->block, st);
+    std::vector<short> hpk((size_t)ni * mp);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(counts, cnt.p, (size_t)ni * sizeof(int), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(hpk.data(), pk.p, hpk.size() * sizeof(short), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    cleanup();
+    CK(e);
+    std::vector<float> hv((size_t)t->P.nvert * 3);
+    if (peak_dirs) CK(cudaMemcpy(hv.data(), t->verts.p, hv.size() * 4, cudaMemcpyDeviceToHost));
+    for (int s = 0; s < ni; s++)
+        for (int k = 0; k < max_peaks; k++) {
+            const int v = (k < counts[s]) ? hpk[(size_t)s * mp + k] : -1;
+            if (peak_vertex) peak_vertex[(size_t)s * max_peaks + k] = v;
+            if (peak_dirs)
+                for (int c = 0; c < 3; c++)
+                    peak_dirs[((size_t)s * max_peaks + k) * 3 + c] = v >= 0 ? hv[3 * v + c] : 0.0f;
+        }
+    return CSL_OK;
+}
+
+int csl_get_direction(csl_tracker *t, const float *points, const float *dirs,
+                      const unsigned long long *subsequence, const unsigned long long *offset,
+                      long long n, float *frames, float *new_dirs, int *ok, int *draws) {
+    if (!t) return fail(nullptr, CSL_E_INVALID, "NULL tracker");
+    if (n < 0 || (n > 0 && (!points || !dirs || !subsequence || !offset || !new_dirs || !ok)))
+        return fail(t, CSL_E_INVALID, "bad arguments");
+    if (t->P.model == PTT && n > 0 && !frames) return fail(t, CSL_E_INVALID, "PTT needs frames");
+    if (n == 0) return CSL_OK;
+    CK(cudaSetDevice(t->device));
+    cudaStream_t st = t->own_stream;
+    const int ni = (int)n;
+    DevBuf<float> pd, dd, fr, od;
+    DevBuf<unsigned long long> sq, of;
+    DevBuf<int> okd, drd;
+    cudaError_t e = cudaSuccess;
+    auto step = [&](cudaError_t x) { if (e == cudaSuccess) e = x; };
+    step(pd.ensure((size_t)ni * 3));
+    step(dd.ensure((size_t)ni * 3));
+    step(fr.ensure((size_t)ni * 9));
+    step(od.ensure((size_t)ni * 3));
+    step(sq.ensure(ni));
+    step(of.ensure(ni));
+    step(okd.ensure(ni));
+    step(drd.ensure(ni));
+    step(cudaMemcpyAsync(pd.p, points, (size_t)ni * 12, cudaMemcpyHostToDevice, st));
+    step(cudaMemcpyAsync(dd.p, dirs, (size_t)ni * 12, cudaMemcpyHostToDevice, st));
+    step(cudaMemcpyAsync(sq.p, subsequence, (size_t)ni * 8, cudaMemcpyHostToDevice, st));
+    step(cudaMemcpyAsync(of.p, offset, (size_t)ni * 8, cudaMemcpyHostToDevice, st));
+    if (frames) step(cudaMemcpyAsync(fr.p, frames, (size_t)ni * 36, cudaMemcpyHostToDevice, st));
+    step(launch_get_direction(t->P, t->partner.p, pd.p, dd.p, sq.p, of.p, ni, fr.p, od.p, okd.p,
+                              drd.p, st));
+    step(cudaMemcpyAsync(new_dirs, od.p, (size_t)ni * 12, cudaMemcpyDeviceToHost, st));
+    step(cudaMemcpyAsync(ok, okd.p, (size_t)ni * 4, cudaMemcpyDeviceToHost, st));
+    if (draws) step(cudaMemcpyAsync(draws, drd.p, (size_t)ni * 4, cudaMemcpyDeviceToHost, st));
+    if (frames) step(cudaMemcpyAsync(frames, fr.p, (size_t)ni * 36, cudaMemcpyDeviceToHost, st));
+    step(cudaStreamSynchronize(st));
+    pd.release(); dd.release(); fr.release(); od.release();
+    sq.release(); of.release(); okd.release(); drd.release();
+    CK(e);
+    return CSL_OK;
+}
+
+int csl_batch_timings(csl_tracker *t, float *ms4, int *pass2_runs) {
+    if (!t) return fail(nullptr, CSL_E_INVALID, "NULL tracker");
+    if (!t->ok_batch) return fail(t, CSL_E_STATE, "no completed batch");
+    if (ms4)
+        for (int i = 0; i < 4; i++) ms4[i] = t->ms[i];
+    if (pass2_runs) *pass2_runs = t->pass2_runs;
+    return CSL_OK;
+}
+
+int csl_device_constants(csl_tracker *t, float *cos_max_angle, float *cos_min_separation) {
+    if (!t) return fail(nullptr, CSL_E_INVALID, "NULL tracker");
+    if (cos_max_angle) *cos_max_angle = t->P.cos_max_angle;
+    if (cos_min_separation) *cos_min_separation = t->P.cos_min_sep;
+    return CSL_OK;
+}
+
+int csl_philox_stream(unsigned long long seed, unsigned long long subsequence,
+                      unsigned long long offset, long long n, unsigned int *out) {
+    csl_tracker *t = nullptr;
+    if (n < 0 || (n > 0 && !out)) return fail(nullptr, CSL_E_INVALID, "bad arguments");
+    if (n == 0) return CSL_OK;
+    DevBuf<unsigned> d;
+    CK(d.ensure(n));
+    cudaError_t e = launch_philox_stream(seed, subsequence, offset, n, d.p, 0);
+    if (e == cudaSuccess) e = cudaMemcpy(out, d.p, (size_t)n * 4, cudaMemcpyDeviceToHost);
+    d.release();
+    CK(e);
+    return CSL_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,505 @@
+// Tracking kernels and their launchers.
+//
+// Pass 1 (seed peaks, one warp per seed) and pass 2 (tracking) follow the
+// reference's two-pass structure (cu_propagate_seeds.py:206-233), with the
+// host-side Python scan replaced by device scans and the padded
+// nSlines x 1002 x float3 output replaced by a point pool plus a final
+// compaction, so only valid points are ever copied off the device.
+//
+// Pass 2 is a persistent kernel: one block per SM slot, each warp takes the
+// next seed from an atomic queue, tracks every peak of that seed (backward,
+// then forward, the RNG stream continuing across them as in
+// genStreamlinesMerge*_k), reserves space in the pool with one atomicAdd
+// and copies the streamline there.  Uneven streamline lengths therefore
+// never idle a warp while work remains.
+#include <cub/device/device_scan.cuh>
+#include <cuda_runtime.h>
+
+#include "boot.cuh"
+#include "common.cuh"
+#include "kernels.h"
+#include "prob.cuh"
+#include "ptt.cuh"
+
+namespace csl {
+
+// ---------------------------------------------------------------------------
+// shared-memory layout
+
+struct WarpBufs {
+    float *odf;     // [n32] ODF / PMF / CDF
+    int *ind;       // [max(n32, samplm_nr)] peak flags / indices
+    float *vox;     // BOOT [n32t]
+    float *msk;     // BOOT [n32t]
+    float *r;       // BOOT [rh]
+    float *h;       // BOOT [rh]
+    float *frame;   // PTT [18]
+    float *face;    // PTT [32]
+    float *vpdf;    // PTT [32]
+};
+
+__host__ __device__ inline int round32(int x) { return (x + 31) / 32 * 32; }
+
+// `track`: pass-2 layout, where PROB and PTT keep the (rarely used) peak
+// index buffer in global scratch so more warps fit on an SM
+__host__ __device__ inline int warp_smem_floats(const DevParams &P, bool track) {
+    const int nr = round32(P.samplm_nr);
+    if (P.model == OPDT || P.model == CSA) {
+        const int n32t = round32(P.dimt);
+        const int rh = n32t > nr ? n32t : nr;
+        return 2 * n32t + 2 * rh + nr;
+    }
+    int f = track ? nr : 2 * nr;
+    if (P.model == PTT) f += 18 + 32 + 32;
+    return f;
+}
+
+__host__ int smem_bytes(const DevParams &P, int warps, bool track) {
+    return (kMaxSortLayers * kWarp) * 4 + warps * warp_smem_floats(P, track) * 4;
+}
+
+__device__ inline WarpBufs carve(const DevParams &P, float *base, int warp, bool track,
+                                 int *global_ind) {
+    WarpBufs b = {};
+    float *p = base + (size_t)warp * warp_smem_floats(P, track);
+    const int nr = round32(P.samplm_nr);
+    if (P.model == OPDT || P.model == CSA) {
+        const int n32t = round32(P.dimt);
+        const int rh = n32t > nr ? n32t : nr;
+        b.vox = p;
+        b.msk = p + n32t;
+        b.r = p + 2 * n32t;
+        b.h = p + 2 * n32t + rh;
+        b.ind = reinterpret_cast<int *>(p + 2 * n32t + 2 * rh);
+        b.odf = b.h;
+    } else {
+        b.odf = p;
+        const int f = track ? nr : 2 * nr;
+        b.ind = track ? global_ind : reinterpret_cast<int *>(p + nr);
+        if (P.model == PTT) {
+            b.frame = p + f;
+            b.face = b.frame + 18;
+            b.vpdf = b.face + 32;
+        }
+    }
+    return b;
+}
+
+__device__ inline void load_partner(const int *__restrict__ g, int *sh) {
+    for (int i = threadIdx.x; i < kMaxSortLayers * kWarp; i += blockDim.x) sh[i] = g[i];
+}
+
+// ---------------------------------------------------------------------------
+// pass 1: initial directions per seed
+
+template <int MODEL>
+__device__ int seed_peaks_dispatch(const DevParams &P, float3 seed, const WarpBufs &W,
+                                   const int *partner_sh, int lane, unsigned long long subseq) {
+    if (MODEL == PROB) return prob_seed_peaks(P, seed, W.odf, W.ind, partner_sh, lane);
+    if (MODEL == PTT) return ptt_seed_peaks(P, seed, W.odf, W.ind, partner_sh, lane);
+    // bootstrap: one attempt with the pass-1 stream (boot.cu:649)
+    Philox rng;
+    rng.init(P.rng_seed, subseq, 0);
+    BootSmem S{W.vox, W.msk, W.r, W.h, W.ind};
+    float3 unused;
+    return boot_get_direction<1, MODEL>(P, rng, make_float3(0, 0, 0), seed, S, partner_sh, lane,
+                                        &unused, nullptr);
+}
+
+template <int MODEL>
+__global__ void __launch_bounds__(256) seed_peaks_kernel(DevParams P, const float *__restrict__ seeds,
+                                                         int n, long long rng_base, const int *partner,
+                                                         int *npeaks, short *peaks, int max_store) {
+    extern __shared__ float smem[];
+    int *partner_sh = reinterpret_cast<int *>(smem);
+    load_partner(partner, partner_sh);
+    __syncthreads();
+    const int warp = threadIdx.x / kWarp, lane = threadIdx.x & 31;
+    const WarpBufs W = carve(P, smem + kMaxSortLayers * kWarp, warp, false, nullptr);
+    const int wpb = blockDim.x / kWarp;
+    for (int s = blockIdx.x * wpb + warp; s < n; s += gridDim.x * wpb) {
+        const float3 seed = make_float3(seeds[3 * s], seeds[3 * s + 1], seeds[3 * s + 2]);
+        const unsigned long long gid = 32ull * (unsigned long long)(s + rng_base) + lane;
+        const int np = seed_peaks_dispatch<MODEL>(P, seed, W, partner_sh, lane, gid);
+        if (lane == 0) npeaks[s] = np;
+        if (peaks)
+            for (int k = lane; k < max_store; k += kWarp)
+                peaks[(size_t)s * max_store + k] = (short)(k < np ? W.ind[k] : -1);
+        __syncwarp();
+    }
+}
+
+// ---------------------------------------------------------------------------
+// pass 2: tracking
+
+template <int MODEL>
+struct RngOf {
+    using T = Philox;
+};
+template <>
+struct RngOf<PTT> {
+    using T = PhiloxN;
+};
+
+__device__ __forceinline__ void store_pt(float *out, int i, float3 p) {
+    out[3 * i] = p.x;
+    out[3 * i + 1] = p.y;
+    out[3 * i + 2] = p.z;
+}
+
+// tracker_d / tracker_boot_d (generate_streamlines_cuda.cu:283-421, boot.cu:725-824)
+template <int MODEL>
+__device__ int track_one(const DevParams &P, typename RngOf<MODEL>::T &rng, float3 seed,
+                         DirState dir, float *frame, float *out, const WarpBufs &W,
+                         const int *partner_sh, int lane) {
+    const int step_frac = (MODEL == PTT) ? P.step_frac : 1;
+    const double ss = P.step_size / step_frac;
+    float3 pt = seed;
+    if (lane == 0) store_pt(out, 0, pt);
+    __syncwarp();
+    int i;
+    const int imax = P.max_sline_len * step_frac;
+    for (i = 1; i < imax; i++) {
+        DirState nd;
+        nd.vtx = -1;
+        nd.neg = 0;
+        int ndir;
+        if constexpr (MODEL == PROB) {
+            ndir = prob_get_direction(P, pt, dir, W.odf, rng, lane, &nd, nullptr);
+        } else if constexpr (MODEL == PTT) {
+            PttSmem S{W.face, W.vpdf};
+            ndir = ptt_get_direction<false>(P, rng, dir.d, frame, pt, S, lane, &nd.d);
+        } else {
+            BootSmem S{W.vox, W.msk, W.r, W.h, W.ind};
+            ndir = boot_get_direction<5, MODEL>(P, rng, dir.d, pt, S, partner_sh, lane, &nd.d,
+                                                nullptr);
+        }
+        __syncwarp();
+        if (ndir == 0) break;
+        dir = nd;
+        pt.x = (float)fma((double)dir.d.x, ss, (double)pt.x);
+        pt.y = (float)fma((double)dir.d.y, ss, (double)pt.y);
+        pt.z = (float)fma((double)dir.d.z, ss, (double)pt.z);
+        if (lane == 0 && (i % step_frac) == 0) store_pt(out, i / step_frac, pt);
+        __syncwarp();
+        if (check_point(P, pt) != TRACKPOINT) break;
+    }
+    int nsteps = i / step_frac;
+    if (((i % step_frac) != 0) && i < step_frac * (P.max_sline_len - 1)) nsteps++;
+    return nsteps;
+}
+
+template <int MODEL>
+__global__ void __launch_bounds__(256, MODEL == PROB ? 2 : 1) track_kernel(DevParams P, BatchArgs B, const int *partner,
+                                                    const int *__restrict__ npeaks,
+                                                    const short *__restrict__ peaks, int max_store,
+                                                    const int *__restrict__ sl_off, int *out_len,
+                                                    int *out_seed, long long *out_src) {
+    extern __shared__ float smem[];
+    int *partner_sh = reinterpret_cast<int *>(smem);
+    load_partner(partner, partner_sh);
+    __syncthreads();
+    const int warp = threadIdx.x / kWarp, lane = threadIdx.x & 31;
+    const size_t gwarp = (size_t)blockIdx.x * (blockDim.x / kWarp) + warp;
+    float *scrB = B.scratch + gwarp * (size_t)scratch_floats_per_warp(P);
+    float *scrF = scrB + (size_t)P.max_sline_len * 3;
+    int *plist = reinterpret_cast<int *>(scrF + (size_t)P.max_sline_len * 3);
+    const WarpBufs W = carve(P, smem + kMaxSortLayers * kWarp, warp, true, plist);
+
+    for (;;) {
+        int s = 0;
+        if (lane == 0) s = atomicAdd(B.queue, 1);
+        s = __shfl_sync(FULL, s, 0);
+        if (s >= B.nseeds) break;
+        const int np = npeaks[s];
+        if (np == 0) continue;
+        const float3 seed = make_float3(B.seeds[3 * s], B.seeds[3 * s + 1], B.seeds[3 * s + 2]);
+        const unsigned long long gid = 32ull * (unsigned long long)(s + B.rng_index_base) + lane;
+        // peak list: stored by pass 1, or recomputed into this warp's scratch
+        const short *stored = peaks + (size_t)s * max_store;
+        if (np > max_store) {
+            seed_peaks_dispatch<MODEL>(P, seed, W, partner_sh, lane, gid);
+            if (W.ind != plist)
+                for (int k = lane; k < np; k += kWarp) plist[k] = W.ind[k];
+        }
+        __syncwarp();
+        typename RngOf<MODEL>::T rng;
+        rng.init(P.rng_seed, gid + 1, 0);
+        const int base = sl_off[s];
+        {
+            for (int k = 0; k < np; k++) {
+                const int pv = (np > max_store) ? plist[k] : (int)stored[k];
+                const float3 fs = vert3(P.verts, pv);
+                int len;
+                int nB = 0, nF = 0;
+                bool single = false;
+                if constexpr (MODEL == PTT) {
+                    PttSmem S{W.face, W.vpdf};
+                    if (!ptt_init_frame(P, rng, fs, seed, W.frame, S, lane)) single = true;
+                }
+                if (single) {
+                    if (lane == 0) store_pt(scrB, 0, seed);
+                    __syncwarp();
+                    nB = 1;
+                    nF = 1;
+                    len = 1;
+                } else {
+                    DirState db{make_float3(-fs.x, -fs.y, -fs.z), pv, 1};
+                    DirState df{fs, pv, 0};
+                    nB = track_one<MODEL>(P, rng, seed, db, W.frame, scrB, W, partner_sh, lane);
+                    nF = track_one<MODEL>(P, rng, seed, df, W.frame + 9, scrF, W, partner_sh,
+                                                 lane);
+                    len = nB - 1 + nF;
+                }
+                __syncwarp();
+                unsigned long long off = 0;
+                if (lane == 0) off = atomicAdd(B.pool_count, (unsigned long long)len);
+                off = __shfl_sync(FULL, off, 0);
+                long long src = -1;
+                if (off + (unsigned long long)len <= B.pool_cap) {
+                    src = (long long)off;
+                    float *dst = B.pool + off * 3;
+                    for (int j = lane; j < len; j += kWarp) {
+                        const float *p = (j < nB) ? scrB + 3 * (nB - 1 - j) : scrF + 3 * (j - nB + 1);
+                        dst[3 * j] = p[0];
+                        dst[3 * j + 1] = p[1];
+                        dst[3 * j + 2] = p[2];
+                    }
+                } else if (lane == 0) {
+                    atomicOr(B.status, ST_POOL_OVERFLOW);
+                }
+                if (lane == 0) {
+                    out_len[base + k] = len;
+                    out_seed[base + k] = s;
+                    out_src[base + k] = src;
+                }
+                __syncwarp();
+            }
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// post-processing: gather pool -> compacted, ordered points
+
+__global__ void gather_kernel(const float *__restrict__ pool, const long long *__restrict__ src,
+                              const int *__restrict__ len, const long long *__restrict__ pt_off,
+                              int nsl, float *__restrict__ out) {
+    const int lane = threadIdx.x & 31;
+    const int wpb = blockDim.x / kWarp;
+    for (int sl = blockIdx.x * wpb + threadIdx.x / kWarp; sl < nsl; sl += gridDim.x * wpb) {
+        const long long s = src[sl];
+        const int n3 = 3 * len[sl];
+        const float *a = pool + 3 * s;
+        float *b = out + 3 * pt_off[sl];
+        for (int j = lane; j < n3; j += kWarp) b[j] = a[j];
+    }
+}
+
+// ---------------------------------------------------------------------------
+// tables and constants
+
+// keep-bit table of the probabilistic cone filter: bit (32c + l) of row
+// (sign, k) is set when vertex 32c+l survives `dot < cos(max_angle)` for the
+// incoming direction (-1)^sign * vertex k (generate_streamlines_cuda.cu:141-152)
+__global__ void cone_mask_kernel(DevParams P, uint32_t *mask) {
+    const int lane = threadIdx.x & 31;
+    const int row = blockIdx.x * (blockDim.x / kWarp) + threadIdx.x / kWarp;
+    if (row >= 2 * P.nvert) return;
+    const int neg = row / P.nvert, k = row % P.nvert;
+    float3 d = vert3(P.verts, k);
+    if (neg) d = make_float3(-d.x, -d.y, -d.z);
+    const float cos_similarity = P.cos_max_angle;
+    for (int ch = 0; ch < P.nch; ch++) {
+        const int t = ch * kWarp + lane;
+        bool keep = false;
+        if (t < P.samplm_nr) {
+            const float3 sv = vert3(P.verts, t);
+            float dot = d.x * sv.x + d.y * sv.y + d.z * sv.z;
+            if (P.sphere_symm) dot = fabsf(dot);
+            keep = !(dot < cos_similarity);
+        }
+        const unsigned b = __ballot_sync(FULL, keep);
+        if (lane == 0) mask[(size_t)row * P.nch + ch] = b;
+    }
+}
+
+__global__ void device_cos_kernel(float a, float b, float *out) {
+    out[0] = __cosf(a);
+    out[1] = __cosf(b);
+}
+
+__global__ void philox_stream_kernel(unsigned long long seed, unsigned long long subseq,
+                                     unsigned long long offset, long long n, unsigned *out) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    Philox g;
+    g.init(seed, subseq, offset);
+    for (long long i = 0; i < n; i++) out[i] = g.next();
+}
+
+// One direction-getter call per query (test entry point).  Query q runs on
+// warp q; lane l uses Philox subsequence subseq[q] + l at offset offs[q]
+// (the reference's per-lane streams), lane 0's draws are counted.
+template <int MODEL>
+__global__ void get_direction_kernel(DevParams P, const int *partner, const float *pts,
+                                     const float *dirs, const unsigned long long *subseq,
+                                     const unsigned long long *offs, int n, float *frames,
+                                     float *out_dirs, int *out_ok, int *out_draws) {
+    extern __shared__ float smem[];
+    int *partner_sh = reinterpret_cast<int *>(smem);
+    load_partner(partner, partner_sh);
+    __syncthreads();
+    const int warp = threadIdx.x / kWarp, lane = threadIdx.x & 31;
+    const WarpBufs W = carve(P, smem + kMaxSortLayers * kWarp, warp, false, nullptr);
+    const int q = blockIdx.x * (blockDim.x / kWarp) + warp;
+    if (q >= n) return;
+    const float3 pt = make_float3(pts[3 * q], pts[3 * q + 1], pts[3 * q + 2]);
+    DirState d{make_float3(dirs[3 * q], dirs[3 * q + 1], dirs[3 * q + 2]), -1, 0};
+    typename RngOf<MODEL>::T rng;
+    rng.init(P.rng_seed, subseq[q] + lane, offs[q]);
+    DirState nd;
+    nd.d = d.d;
+    nd.vtx = -1;
+    nd.neg = 0;
+    int ok = 0, draws = 0;
+    if constexpr (MODEL == PROB) {
+        ok = prob_get_direction(P, pt, d, W.odf, rng, lane, &nd, &draws);
+    } else if constexpr (MODEL == PTT) {
+        if (lane < 9) W.frame[lane] = frames[9 * q + lane];
+        __syncwarp();
+        PttSmem S{W.face, W.vpdf};
+        ok = ptt_get_direction<false>(P, rng, d.d, W.frame, pt, S, lane, &nd.d);
+        __syncwarp();
+        if (lane < 9) frames[9 * q + lane] = W.frame[lane];
+    } else {
+        BootSmem S{W.vox, W.msk, W.r, W.h, W.ind};
+        ok = boot_get_direction<5, MODEL>(P, rng, d.d, pt, S, partner_sh, lane, &nd.d, &draws);
+    }
+    if (lane == 0) {
+        out_dirs[3 * q] = nd.d.x;
+        out_dirs[3 * q + 1] = nd.d.y;
+        out_dirs[3 * q + 2] = nd.d.z;
+        out_ok[q] = ok;
+        if (out_draws) out_draws[q] = draws;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// launchers
+
+#define CSL_DISPATCH_MODEL(model, ...)                      \
+    switch (model) {                                         \
+        case OPDT: { constexpr int M = OPDT; __VA_ARGS__; } break;  \
+        case CSA: { constexpr int M = CSA; __VA_ARGS__; } break;    \
+        case PROB: { constexpr int M = PROB; __VA_ARGS__; } break;  \
+        default: { constexpr int M = PTT; __VA_ARGS__; } break;     \
+    }
+
+template <typename K>
+static cudaError_t set_smem(K kernel, int bytes) {
+    return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+}
+
+cudaError_t launch_seed_peaks(const DevParams &P, const float *seeds, int n, long long rng_base,
+                              const int *partner, int *npeaks, short *peaks, int max_store,
+                              int grid, int block, cudaStream_t st) {
+    const int smem = smem_bytes(P, block / kWarp, false);
+    cudaError_t e = cudaSuccess;
+    CSL_DISPATCH_MODEL(P.model, {
+        e = set_smem(seed_peaks_kernel<M>, smem);
+        if (e != cudaSuccess) return e;
+        seed_peaks_kernel<M><<<grid, block, smem, st>>>(P, seeds, n, rng_base, partner, npeaks,
+                                                        peaks, max_store);
+    });
+    return cudaGetLastError();
+}
+
+cudaError_t track_occupancy(const DevParams &P, int block, int *blocks_per_sm) {
+    const int smem = smem_bytes(P, block / kWarp, true);
+    cudaError_t e = cudaSuccess;
+    CSL_DISPATCH_MODEL(P.model, {
+        e = set_smem(track_kernel<M>, smem);
+        if (e != cudaSuccess) return e;
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, track_kernel<M>, block,
+                                                          smem);
+    });
+    return e;
+}
+
+cudaError_t launch_track(const DevParams &P, const BatchArgs &B, const int *partner,
+                         const int *npeaks, const short *peaks, int max_store, const int *sl_off,
+                         int *out_len, int *out_seed, long long *out_src, int grid, int block,
+                         cudaStream_t st) {
+    const int smem = smem_bytes(P, block / kWarp, true);
+    cudaError_t e = cudaSuccess;
+    CSL_DISPATCH_MODEL(P.model, {
+        e = set_smem(track_kernel<M>, smem);
+        if (e != cudaSuccess) return e;
+        track_kernel<M><<<grid, block, smem, st>>>(P, B, partner, npeaks, peaks, max_store, sl_off,
+                                                   out_len, out_seed, out_src);
+    });
+    return cudaGetLastError();
+}
+
+cudaError_t launch_get_direction(const DevParams &P, const int *partner, const float *pts,
+                                 const float *dirs, const unsigned long long *subseq,
+                                 const unsigned long long *offs, int n, float *frames,
+                                 float *out_dirs, int *out_ok, int *out_draws, cudaStream_t st) {
+    const int block = 128;
+    const int smem = smem_bytes(P, block / kWarp, false);
+    const int grid = (n + 3) / 4;
+    cudaError_t e = cudaSuccess;
+    CSL_DISPATCH_MODEL(P.model, {
+        e = set_smem(get_direction_kernel<M>, smem);
+        if (e != cudaSuccess) return e;
+        get_direction_kernel<M><<<grid, block, smem, st>>>(P, partner, pts, dirs, subseq, offs, n,
+                                                           frames, out_dirs, out_ok, out_draws);
+    });
+    return cudaGetLastError();
+}
+
+cudaError_t launch_gather(const float *pool, const long long *src, const int *len,
+                          const long long *pt_off, int nsl, float *out, int grid, cudaStream_t st) {
+    if (nsl <= 0) return cudaSuccess;
+    gather_kernel<<<grid, 256, 0, st>>>(pool, src, len, pt_off, nsl, out);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_cone_mask(const DevParams &P, uint32_t *mask, cudaStream_t st) {
+    const int rows = 2 * P.nvert;
+    cone_mask_kernel<<<(rows + 7) / 8, 256, 0, st>>>(P, mask);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_device_cos(float a, float b, float *out, cudaStream_t st) {
+    device_cos_kernel<<<1, 1, 0, st>>>(a, b, out);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_philox_stream(unsigned long long seed, unsigned long long subseq,
+                                 unsigned long long offset, long long n, unsigned *out,
+                                 cudaStream_t st) {
+    philox_stream_kernel<<<1, 32, 0, st>>>(seed, subseq, offset, n, out);
+    return cudaGetLastError();
+}
+
+cudaError_t scan_temp_bytes(int n, size_t *bytes) {
+    size_t a = 0, b = 0;
+    cudaError_t e = cub::DeviceScan::ExclusiveSum(nullptr, a, (const int *)nullptr, (int *)nullptr, n + 1);
+    if (e != cudaSuccess) return e;
+    e = cub::DeviceScan::ExclusiveSum(nullptr, b, (const int *)nullptr, (long long *)nullptr, n + 1);
+    *bytes = a > b ? a : b;
+    return e;
+}
+
+cudaError_t exclusive_scan_i32(void *tmp, size_t tmp_bytes, const int *in, int *out, int n,
+                               cudaStream_t st) {
+    return cub::DeviceScan::ExclusiveSum(tmp, tmp_bytes, in, out, n, st);
+}
+
+cudaError_t exclusive_scan_i64(void *tmp, size_t tmp_bytes, const int *in, long long *out, int n,
+                               cudaStream_t st) {
+    return cub::DeviceScan::ExclusiveSum(tmp, tmp_bytes, in, out, n, st);
+}
+
+}  // namespace csl

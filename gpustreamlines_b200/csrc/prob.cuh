@@ -1,0 +1,162 @@
+// Probabilistic direction getter (generate_streamlines_cuda.cu:54-275).
+//
+// Per step: trilinear PMF gather (lane l owns vertices l, l+32, ...), absolute threshold at PMF_THRESHOLD_P * max, cone filter,
+// reference-order inclusive scan, one Philox uniform drawn by lane 0, the
+// reference's bisection + ballot search, and the hemisphere flip.
+//
+// The cone filter reads a precomputed keep-bit table instead of evaluating
+// 3 * V multiply-adds per step: along a streamline the incoming direction is
+// always +/- a sphere vertex (pass-1 peaks and every sampled step are
+// vertices), and the table bits are produced on the device with the same dot
+// product expression, so the filter is bit-identical.
+#pragma once
+#include "common.cuh"
+
+namespace csl {
+
+// Direction state along a streamline: the float3 plus, when it is exactly
+// +/- a sphere vertex, that vertex and the sign (vtx < 0: arbitrary vector).
+struct DirState {
+    float3 d;
+    int vtx;
+    int neg;
+};
+
+__device__ __forceinline__ int prob_get_direction(const DevParams &P, float3 pt, DirState dir,
+                                                  float *cdf_sh, Philox &rng, int lane,
+                                                  DirState *out, int *ndraws) {
+    Corners c;
+    if (!trilinear_setup(P, pt, c)) return 0;
+    const int len = P.samplm_nr;
+    const int nch = P.nch;
+    const float *rows[8];
+#pragma unroll
+    for (int q = 0; q < 8; q++) rows[q] = P.dataf + c.base[q];
+
+    // gather (4 chunks of 32 vertices in flight per lane) + running max
+    float m = -FLT_MAX;
+    int ch = 0;
+    for (; ch + 4 <= nch; ch += 4) {
+        float a[4];
+#pragma unroll
+        for (int u = 0; u < 4; u++) {
+            const int t = (ch + u) * kWarp + lane;
+            float acc = 0.0f;
+            if (t < len) {
+#pragma unroll
+                for (int q = 0; q < 8; q++) acc += c.w[q] * __ldg(rows[q] + t);
+            }
+            a[u] = acc;
+        }
+#pragma unroll
+        for (int u = 0; u < 4; u++) {
+            const int t = (ch + u) * kWarp + lane;
+            if (t < len) {
+                cdf_sh[t] = a[u];
+                m = fmax_ref(m, a[u]);
+            }
+        }
+    }
+    for (; ch < nch; ch++) {
+        const int t = ch * kWarp + lane;
+        if (t < len) {
+            float acc = 0.0f;
+#pragma unroll
+            for (int q = 0; q < 8; q++) acc += c.w[q] * __ldg(rows[q] + t);
+            cdf_sh[t] = acc;
+            m = fmax_ref(m, acc);
+        }
+    }
+    m = warp_max_ref(m);
+    const float thr = (float)(P.pmf_threshold * (double)m);
+    __syncwarp();
+
+    // threshold + cone filter + reference-order scan, chunk by chunk
+    const uint32_t *row = (dir.vtx >= 0)
+                              ? P.cone_mask + ((size_t)dir.neg * P.nvert + dir.vtx) * nch
+                              : nullptr;
+    const float cos_similarity = P.cos_max_angle;
+    float carry = 0.0f;
+    for (ch = 0; ch < nch; ch++) {
+        const int t = ch * kWarp + lane;
+        const bool valid = t < len;
+        float x = valid ? cdf_sh[t] : 0.0f;
+        bool keep;
+        if (row) {
+            keep = (__ldg(row + ch) >> lane) & 1u;
+        } else {
+            keep = true;
+            if (valid) {
+                const float3 sv = vert3(P.verts, t);
+                float dot = dir.d.x * sv.x + dir.d.y * sv.y + dir.d.z * sv.z;
+                if (P.sphere_symm) dot = fabsf(dot);
+                keep = !(dot < cos_similarity);
+            }
+        }
+        if (x < thr || !keep) x = 0.0f;
+        if (lane == 0 && ch != 0) x = x + carry;
+#pragma unroll
+        for (int i = 1; i < kWarp; i <<= 1) {
+            const float y = __shfl_up_sync(FULL, x, i);
+            if (lane >= i && valid) x += y;
+        }
+        if (valid) cdf_sh[t] = x;
+        carry = __shfl_sync(FULL, x, 31);
+    }
+    __syncwarp();
+    const float last_cdf = cdf_sh[len - 1];
+    if (last_cdf == 0) return 0;
+
+    float sel = 0.0f;
+    if (lane == 0) sel = rng.uniform() * last_cdf;
+    sel = __shfl_sync(FULL, sel, 0);
+    if (ndraws) *ndraws += 1;
+
+    int low = 0, high = len - 1;
+    while ((high - low) >= kWarp) {
+        const int mid = (low + high) / 2;
+        if (cdf_sh[mid] < sel)
+            low = mid;
+        else
+            high = mid;
+    }
+    const bool b = (low + lane <= high) ? (sel < cdf_sh[low + lane]) : false;
+    const unsigned msk = __ballot_sync(FULL, b);
+    int ind = low + __ffs(msk) - 1;
+    // The reference reads vertex[-1] in this (measure-zero) case; stay in bounds.
+    if (ind < 0) ind = 0;
+    __syncwarp();
+
+    const float3 sv = vert3(P.verts, ind);
+    if ((dir.d.x * sv.x + dir.d.y * sv.y + dir.d.z * sv.z) > 0) {
+        out->d = sv;
+        out->neg = 0;
+    } else {
+        out->d = make_float3(-sv.x, -sv.y, -sv.z);
+        out->neg = 1;
+    }
+    out->vtx = ind;
+    return 1;
+}
+
+// Pass-1 peaks at a seed (getNumStreamlinesProb_k, generate_streamlines_cuda.cu:427-462).
+__device__ __forceinline__ int prob_seed_peaks(const DevParams &P, float3 seed, float *odf_sh,
+                                               int *ind_sh, const int *partner_sh, int lane) {
+    Corners c;
+    if (!trilinear_setup(P, seed, c)) return 0;
+    const int len = P.samplm_nr;
+    float m = -FLT_MAX;
+    for (int t = lane; t < len; t += kWarp) {
+        const float x = trilinear_elem(P.dataf, c, t);
+        odf_sh[t] = x;
+        m = fmax_ref(m, x);
+    }
+    m = warp_max_ref(m);
+    const float thr = (float)(P.pmf_threshold * (double)m);
+    for (int t = lane; t < len; t += kWarp)
+        if (odf_sh[t] < thr) odf_sh[t] = 0.0f;
+    __syncwarp();
+    return peak_directions(P, odf_sh, ind_sh, len, partner_sh, lane);
+}
+
+}  // namespace csl

@@ -1,0 +1,197 @@
+/*
+ * gpustreamlines_b200 -- C ABI of the B200 streamline tracker.
+ *
+ * The reference (dipy/GPUStreamlines, package `cuslines`) has no C ABI: its
+ * Python host code JIT-compiles the kernels with NVRTC and launches them with
+ * raw device pointers in a fixed argument order
+ * (cuslines/cuda_python/cu_direction_getters.py:313-364, 381-414, 632-648).
+ * Each entry point below names the reference interface it replaces.
+ *
+ * Conventions
+ *  - Every function returns an int status: 0 (CSL_OK) on success, a negative
+ *    CSL_E* code otherwise.  Nothing in the library calls exit().
+ *  - The caller owns every host buffer; the library owns every device buffer
+ *    it allocates.  One tracker handle is bound to one CUDA device.
+ *  - A handle is not thread safe (the reference drives all GPUs from one host
+ *    thread, cu_propagate_seeds.py:45-54).
+ *  - Arrays are C-order float32 unless stated otherwise.  Seeds and points are
+ *    voxel coordinates [n,3].
+ */
+#ifndef GPUSTREAMLINES_B200_H
+#define GPUSTREAMLINES_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define CSL_OK 0
+#define CSL_E_INVALID (-1)   /* bad argument or shape (ValueError in the reference) */
+#define CSL_E_CUDA (-2)      /* a CUDA runtime call failed (RuntimeError in the reference) */
+#define CSL_E_NOMEM (-3)     /* device allocation failed */
+#define CSL_E_STATE (-4)     /* call out of order (e.g. fetch before propagate) */
+#define CSL_E_KERNEL (-5)    /* a kernel reported an error status */
+
+/* Model / direction-getter kinds (cuslines/cuda_c/globals.h:82-87). */
+#define CSL_MODEL_OPDT 0
+#define CSL_MODEL_CSA 1
+#define CSL_MODEL_PROB 2
+#define CSL_MODEL_PTT 3
+
+typedef struct csl_tracker csl_tracker;
+
+/*
+ * Tracking parameters.  Replaces the compile-time macro set the reference
+ * builds per tracker (cu_direction_getters.py:70-107, 456-468); here they are
+ * runtime values, so one loaded library serves any volume.
+ * Floating-point parameters are doubles holding the float32-rounded value the
+ * reference passes (it stores REAL_DTYPE(x), cu_tractography.py:149-153).
+ */
+typedef struct csl_params {
+    int model;                    /* CSL_MODEL_* */
+    int dimx, dimy, dimz, dimt;   /* data volume [X,Y,Z,T] */
+    int nvertices;                /* sphere vertices V (== dimt for PROB/PTT) */
+    int nedges;                   /* sphere edges E */
+    int samplm_nr;                /* ODF samples: rows of sampling_matrix (BOOT) or dimt */
+    int sphere_symm;              /* SPHERE_SYMM */
+    int max_sline_len;            /* MAX_SLINE_LEN, 501 in the reference (_globals.py:3) */
+    int _pad0;
+    double step_size;             /* STEP_SIZE, voxels */
+    double max_angle;             /* MAX_ANGLE, radians */
+    double tc_threshold;          /* TC_THRESHOLD */
+    double relative_peak_thresh;  /* RELATIVE_PEAK_THRESH */
+    double min_separation_angle;  /* MIN_SEPARATION_ANGLE, radians */
+    double pmf_threshold;         /* PMF_THRESHOLD_P, 0.05 (_globals.py:4) */
+    unsigned long long rng_seed;  /* RNG_SEED */
+    /* bootstrap getter (BootDirectionGetter, cu_direction_getters.py:147-175) */
+    double min_signal;
+    int delta_nr;                 /* rows of delta_b / delta_q (SH coefficients) */
+    int _pad1;
+    /* PTT getter (PttDirectionGetter, cu_direction_getters.py:417-468) */
+    int odf_lut_res;              /* nearest-vertex LUT resolution (128) */
+    int step_frac;                /* STEP_FRAC = round(step / target_short_step) */
+    double probe_step_size;       /* PROBE_STEP_SIZE (probe_length) */
+    double probe_quality;         /* PROBE_QUALITY */
+    double max_curvature;         /* MAX_CURVATURE = 8 sin(max_angle / 2) */
+    int tile_log2_x, tile_log2_y; /* PTT ODF texture tiling (LOG2_X, LOG2_Y) */
+    int tile_nx, tile_ny, tile_nz;/* tiles per axis (nx, ny, nz) */
+    int _pad2;
+} csl_params;
+
+/*
+ * Host input arrays, uploaded once by csl_create (replaces GPUTracker._allocate
+ * and the getters' allocate_on_gpu, cu_tractography.py:189-258,
+ * cu_direction_getters.py:217-280, 470-517).
+ */
+typedef struct csl_inputs {
+    const float *dataf;           /* [X,Y,Z,T]: DWI (BOOT) or PMF/ODF (PROB); NULL for PTT */
+    const float *stop_map;        /* [X,Y,Z] stopping metric (e.g. FA) */
+    const float *vertices;        /* [V,3] sphere vertices */
+    const int *edges;             /* [E,2] sphere edges */
+    /* BOOT only (NULL otherwise) */
+    const float *H;               /* [hr,hr] hat matrix over the non-b0 volumes */
+    const float *R;               /* [hr,hr] leveraged centred residual matrix */
+    const float *delta_b;         /* [delta_nr,hr] */
+    const float *delta_q;         /* [delta_nr,hr] */
+    const float *sampling_matrix; /* [samplm_nr,delta_nr] */
+    const int *b0s_mask;          /* [T] 1 where the volume is a b0 */
+    /* PTT only (NULL otherwise) */
+    const float *ptt_odf_tiled;   /* [nz*Z, ny*Y, nx*X] tiled, normalised ODF texture data */
+    const float *ptt_lut;         /* [res,res,res] nearest-vertex index, stored as float */
+} csl_inputs;
+
+/* Create a tracker on `device`: validate, upload inputs, build textures and
+ * tables.  Replaces GPUTracker.__init__/_allocate + compile_program
+ * (cu_tractography.py:37-258, cu_direction_getters.py:53-144). */
+int csl_create(const csl_params *params, const csl_inputs *inputs, int device,
+               csl_tracker **out);
+
+/* Release every device resource of the tracker.  Replaces GPUTracker.__exit__
+ * (cu_tractography.py:260-300). */
+int csl_destroy(csl_tracker *t);
+
+/*
+ * Track one batch of seeds held in HOST memory [n,3]: upload, then the fused
+ * seed-peak + tracking kernel, then the device-side exclusive scans and
+ * compaction.  Returns when the results are complete.  Replaces
+ * SeedBatchPropagator.propagate (cu_propagate_seeds.py:206-233), i.e. pass 1
+ * (getNumStreamlines*_k), the host scan (_cumsum_offsets, :95-129) and pass 2
+ * (genStreamlinesMerge*_k).
+ * `rng_index_base` is added to the batch-local seed index before it selects
+ * the Philox subsequence; 0 reproduces the reference, whose kernels index
+ * streams by the chunk-local seed id (generate_streamlines_cuda.cu:498-500).
+ * `stream` is a cudaStream_t (NULL = the tracker's own stream).
+ */
+int csl_propagate(csl_tracker *t, const float *seeds_host, long long n,
+                  long long rng_index_base, void *stream);
+
+/* As csl_propagate, with the seeds already in device memory of the tracker's
+ * device ([n,3] float32).  Results stay on the device until csl_fetch. */
+int csl_propagate_device(csl_tracker *t, const float *seeds_dev, long long n,
+                         long long rng_index_base, void *stream);
+
+/* Number of streamlines and of points of the last batch.  Replaces reading
+ * SeedBatchPropagator.nSlines / sline_lens (cu_propagate_seeds.py:120,235-243). */
+int csl_counts(csl_tracker *t, long long *n_streamlines, long long *n_points);
+
+/*
+ * Copy the last batch's compacted results to host buffers (any may be NULL):
+ *   lengths    int32 [n_streamlines]   points per streamline (slineLen)
+ *   seed_index int32 [n_streamlines]   batch-local seed id (slineSeed)
+ *   points     float32 [n_points,3]    streamlines back to back, in order
+ * Replaces _cleanup's D2H copy of the padded nSlines x 1002 x float3 buffer
+ * (cu_propagate_seeds.py:171-204); only the valid points cross PCIe.
+ */
+int csl_fetch(csl_tracker *t, int *lengths, int *seed_index, float *points);
+
+/* Device pointers of the last batch's compacted results (valid until the next
+ * propagate or destroy); any output may be NULL. */
+int csl_device_results(csl_tracker *t, const int **lengths, const int **seed_index,
+                       const long long **point_offsets, const float **points);
+
+/*
+ * Pass 1 only: number of initial directions per seed and their sphere-vertex
+ * indices, as getNumStreamlines*_k computes them (boot.cu:614-718,
+ * generate_streamlines_cuda.cu:427-462, ptt_init.cu:5-63).  Host buffers:
+ * counts int32 [n]; peak_vertex int32 [n, max_peaks] (-1 padded, may be NULL);
+ * peak_dirs float32 [n, max_peaks, 3] (may be NULL).
+ */
+int csl_seed_peaks(csl_tracker *t, const float *seeds_host, long long n, int max_peaks,
+                   int *counts, int *peak_vertex, float *peak_dirs);
+
+/*
+ * One direction-getter call per query at a fixed position, incoming direction
+ * and Philox state (subsequence, offset), as the tracking step loop makes it
+ * (get_direction_prob_d / get_direction_boot_d / get_direction_ptt_d).
+ * For PTT the 9-float frame per query is read from/written to `frames`.
+ * Outputs: new_dirs float32 [n,3], ok int32 [n] (the getter's return value),
+ * draws int32 [n] (Philox draws consumed by lane 0, may be NULL).
+ */
+int csl_get_direction(csl_tracker *t, const float *points, const float *dirs,
+                      const unsigned long long *subsequence, const unsigned long long *offset,
+                      long long n, float *frames, float *new_dirs, int *ok, int *draws);
+
+/* Device-side durations (ms, CUDA events on the batch's stream) of the last
+ * batch: [0] pass 1 + peak-count scan, [1] host sizing gap, [2] pass 2 (the
+ * tracking kernel, last run), [3] length scan + compaction; pass2_runs is 1,
+ * or 2 when the point pool had to grow.  The reference has no equivalent. */
+int csl_batch_timings(csl_tracker *t, float *ms4, int *pass2_runs);
+
+/* Values the kernels derive on the device: cos(max_angle) and
+ * cos(min_separation_angle) as the tracker uses them. */
+int csl_device_constants(csl_tracker *t, float *cos_max_angle, float *cos_min_separation);
+
+/* Raw Philox4x32-10 stream of this library (curand_init(seed, subsequence,
+ * offset) semantics): out uint32 [n]. */
+int csl_philox_stream(unsigned long long seed, unsigned long long subsequence,
+                      unsigned long long offset, long long n, unsigned int *out);
+
+/* Last error message of the handle (or of the library when t is NULL). */
+int csl_last_error(const csl_tracker *t, char *buf, int buflen);
+
+/* Library version string. */
+const char *csl_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* GPUSTREAMLINES_B200_H */
