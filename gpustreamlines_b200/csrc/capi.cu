@@ -75,6 +75,7 @@ struct csl_tracker {
     DevBuf<unsigned long long> pool_count;
     DevBuf<float> pool, scratch, points;
     DevBuf<unsigned char> scan_tmp;
+    long long *host_stage = nullptr;  // pinned 16-byte staging for the two totals
     long long last_n = -1, nsl = 0, npts = 0;
     int ok_batch = 0;
     cudaStream_t last_stream = nullptr;
@@ -204,6 +205,8 @@ static void release_all(csl_tracker *t) {
     t->scan_tmp.release();
     for (auto &e : t->ev)
         if (e) cudaEventDestroy(e);
+    if (t->host_stage) cudaFreeHost(t->host_stage);
+    t->host_stage = nullptr;
     if (t->own_stream) cudaStreamDestroy(t->own_stream);
     t->own_stream = nullptr;
 }
@@ -390,6 +393,7 @@ int csl_create(const csl_params *params, const csl_inputs *inputs, int device, c
                             smem_bytes(P, t->block / kWarp, true));
         }
         for (auto &e : t->ev) CK(cudaEventCreate(&e));
+        CK(cudaMallocHost(&t->host_stage, 2 * sizeof(long long)));
         CK(t->queue.ensure(1));
         CK(t->status.ensure(1));
         CK(t->pool_count.ensure(1));
@@ -434,7 +438,7 @@ static int run_batch(csl_tracker *t, const float *seeds_dev, long long n, long l
     CK(t->sl_off.ensure(ni + 1));
     CK(t->peaks.ensure((size_t)ni * kMaxStoredPeaksPerSeed));
     size_t tmpb = 0;
-    CK(scan_temp_bytes(std::max(ni, 1 << 20), &tmpb));
+    CK(scan_temp_bytes(ni + 1, &tmpb));
     CK(t->scan_tmp.ensure(tmpb));
 
     // pass 1
@@ -446,9 +450,10 @@ static int run_batch(csl_tracker *t, const float *seeds_dev, long long n, long l
                          kMaxStoredPeaksPerSeed, grid1, t->block, st));
     CK(exclusive_scan_i32(t->scan_tmp.p, t->scan_tmp.cap, t->npeaks.p, t->sl_off.p, ni + 1, st));
     CK(cudaEventRecord(t->ev[1], st));
-    int nsl = 0;
-    CK(cudaMemcpyAsync(&nsl, t->sl_off.p + ni, sizeof(int), cudaMemcpyDeviceToHost, st));
+    int *nsl_h = reinterpret_cast<int *>(t->host_stage);
+    CK(cudaMemcpyAsync(nsl_h, t->sl_off.p + ni, sizeof(int), cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
+    const int nsl = *nsl_h;
     t->nsl = nsl;
     CK(t->out_len.ensure((size_t)nsl + 1));
     CK(t->out_seed.ensure((size_t)nsl + 1));
@@ -481,11 +486,12 @@ static int run_batch(csl_tracker *t, const float *seeds_dev, long long n, long l
                         t->sl_off.p, t->out_len.p, t->out_seed.p, t->out_src.p, grid2, t->block, st));
         CK(cudaEventRecord(t->ev[3], st));
         t->pass2_runs++;
-        int status = 0;
-        unsigned long long used = 0;
-        CK(cudaMemcpyAsync(&status, t->status.p, sizeof(int), cudaMemcpyDeviceToHost, st));
-        CK(cudaMemcpyAsync(&used, t->pool_count.p, sizeof(used), cudaMemcpyDeviceToHost, st));
+        CK(cudaMemcpyAsync(t->host_stage, t->status.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+        CK(cudaMemcpyAsync(t->host_stage + 1, t->pool_count.p, sizeof(unsigned long long),
+                           cudaMemcpyDeviceToHost, st));
         CK(cudaStreamSynchronize(st));
+        const int status = (int)(t->host_stage[0] & 0xffffffff);
+        const unsigned long long used = (unsigned long long)t->host_stage[1];
         if (!(status & ST_POOL_OVERFLOW)) break;
         if (attempt == 1) return fail(t, CSL_E_KERNEL, "point pool overflow after resize");
         want = used + used / 8 + 1024;
@@ -493,10 +499,15 @@ static int run_batch(csl_tracker *t, const float *seeds_dev, long long n, long l
 
     // compaction
     CK(cudaMemsetAsync(t->out_len.p + nsl, 0, sizeof(int), st));
+    CK(scan_temp_bytes(nsl + 1, &tmpb));
+    if (tmpb > t->scan_tmp.cap) {
+        CK(cudaStreamSynchronize(st));
+        CK(t->scan_tmp.ensure(tmpb));
+    }
     CK(exclusive_scan_i64(t->scan_tmp.p, t->scan_tmp.cap, t->out_len.p, t->pt_off.p, nsl + 1, st));
-    long long npts = 0;
-    CK(cudaMemcpyAsync(&npts, t->pt_off.p + nsl, sizeof(long long), cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(t->host_stage, t->pt_off.p + nsl, sizeof(long long), cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
+    const long long npts = t->host_stage[0];
     t->npts = npts;
     CK(t->points.ensure((size_t)npts * 3 + 3));
     CK(launch_gather(t->pool.p, t->out_src.p, t->out_len.p, t->pt_off.p, nsl, t->points.p,

@@ -483,23 +483,26 @@ cudaError_t launch_philox_stream(unsigned long long seed, unsigned long long sub
     return cudaGetLastError();
 }
 
+// temporary storage for an n-element exclusive scan (either output type)
 cudaError_t scan_temp_bytes(int n, size_t *bytes) {
     size_t a = 0, b = 0;
-    cudaError_t e = cub::DeviceScan::ExclusiveSum(nullptr, a, (const int *)nullptr, (int *)nullptr, n + 1);
+    cudaError_t e = cub::DeviceScan::ExclusiveSum(nullptr, a, (const int *)nullptr, (int *)nullptr, n);
     if (e != cudaSuccess) return e;
-    e = cub::DeviceScan::ExclusiveSum(nullptr, b, (const int *)nullptr, (long long *)nullptr, n + 1);
+    e = cub::DeviceScan::ExclusiveSum(nullptr, b, (const int *)nullptr, (long long *)nullptr, n);
     *bytes = a > b ? a : b;
     return e;
 }
 
 cudaError_t exclusive_scan_i32(void *tmp, size_t tmp_bytes, const int *in, int *out, int n,
                                cudaStream_t st) {
-    return cub::DeviceScan::ExclusiveSum(tmp, tmp_bytes, in, out, n, st);
+    cudaError_t e = cub::DeviceScan::ExclusiveSum(tmp, tmp_bytes, in, out, n, st);
+    return e != cudaSuccess ? e : cudaGetLastError();
 }
 
 cudaError_t exclusive_scan_i64(void *tmp, size_t tmp_bytes, const int *in, long long *out, int n,
                                cudaStream_t st) {
-    return cub::DeviceScan::ExclusiveSum(tmp, tmp_bytes, in, out, n, st);
+    cudaError_t e = cub::DeviceScan::ExclusiveSum(tmp, tmp_bytes, in, out, n, st);
+    return e != cudaSuccess ? e : cudaGetLastError();
 }
 
 }  // namespace csl

@@ -67,15 +67,17 @@ struct PhiloxN {
             has_cached = 0;
             return cached;
         }
-        // textbook form: X = sqrt(-2 ln U1) cos(2 pi U2), Y = sqrt(-2 ln U1) sin(2 pi U2)
+        // Box-Muller pair r sin(2 pi U2), r cos(2 pi U2) with r = sqrt(-2 ln U1); the
+        // sine value is returned first (the order the toolkit generator's
+        // streams show, pinned by the GPU tests)
         const float u1 = Philox::uint_to_uniform(g.next());
         const float u2 = Philox::uint_to_uniform(g.next());
         const float r = sqrtf(-2.0f * logf(u1));
         float sn, cs;
         sincospif(2.0f * u2, &sn, &cs);
-        cached = r * sn;
+        cached = r * cs;
         has_cached = 1;
-        return r * cs;
+        return r * sn;
     }
 };
 

@@ -243,6 +243,8 @@ class Reference:
         nsl = self.L.ref_track(*args)
         if nsl < 0:
             raise RuntimeError(f"reference kernels failed ({nsl})")
+        if boot:  # pass 1 only: the reference's bootstrap pass 2 is not launched
+            return counts, None, None, None
         if nsl > cap:
             return self.track(inp, seeds, cap=int(nsl) + 16, ptt=ptt)
         sl_seed, sl_len = sl_seed[:nsl], sl_len[:nsl]

@@ -295,8 +295,9 @@ static int check_point(const orc_params *P, const float p[3]) {
 }
 
 static float dot3(const float a[3], const float *b) {
-    /* a.x*b.x + a.y*b.y + a.z*b.z as contracted by the CUDA compiler */
-    return fmaf(a[2], b[2], fmaf(a[1], b[1], a[0] * b[0]));
+    /* a.x*b.x + a.y*b.y + a.z*b.z as the CUDA compiler contracts it
+     * (pinned on the GPU: tests/test_gpu_parity.py::test_dot_contraction_matches_oracle) */
+    return fmaf(a[2], b[2], fmaf(a[0], b[0], a[1] * b[1]));
 }
 
 /* peak_directions_d: odf [nr] -> kept peak vertex indices in ind[0..n) */

@@ -160,6 +160,15 @@ extern "C" long long ref_track(const float *seeds, int n, const float *dataf, co
         nsl += c;
     }
     off[n] = (int)nsl;
+#if REF_MODEL == 0 || REF_MODEL == 1
+    // The reference's bootstrap pass 2 (genStreamlinesMergeBoot_k) is not
+    // launched: it faulted with an illegal memory access on this pool.  By
+    // reading: its tracking step hands peak_directions_d a one-element shared
+    // slot (__sh_new_dir + tidy, boot.cu:773) and every peak after the first
+    // is written past it (tracking_helpers.cu:220-226), over shared arrays that
+    // hold vertex indices.  Only pass 1 (getNumStreamlinesBoot_k) runs here.
+    goto done;
+#endif
     if (nsl > cap || nsl == 0) goto done;
     {
         REF_CK(cudaMemcpy(offs_d, off.data(), sizeof(int) * (n + 1), cudaMemcpyHostToDevice));
@@ -177,14 +186,6 @@ extern "C" long long ref_track(const float *seeds, int n, const float *dataf, co
                                   const cudaTextureObject_t *__restrict__, float, float3>
             <<<grid, block>>>(0, n, seeds_d, odf_tex_d, stop_tex_d, lut_tex_d, edges_d, offs_d, shdir_d,
                               seed_d, len_d, sl_d);
-#else
-        REF_CK(cudaFuncSetAttribute(
-            genStreamlinesMergeBoot_k<THR_X_SL, THR_X_BL / THR_X_SL, (ModelType)REF_MODEL, float, float3>,
-            cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn));
-        genStreamlinesMergeBoot_k<THR_X_SL, THR_X_BL / THR_X_SL, (ModelType)REF_MODEL, float, float3>
-            <<<grid, block, dyn>>>(0, n, seeds_d, dataf_d, stop_tex_d, (float3 *)verts_d, edges_d,
-                                   min_signal, delta_nr, H_d, R_d, db_d, dq_d, smp_d, b0_d, offs_d,
-                                   shdir_d, seed_d, len_d, sl_d);
 #endif
         REF_CK(cudaGetLastError());
         REF_CK(cudaDeviceSynchronize());

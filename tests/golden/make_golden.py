@@ -7,7 +7,8 @@ The fixtures pin the CPU oracle to the reference and to the CUDA toolkit:
   dot.npz         the reference's 3-term dot expression compiled with --use_fast_math
   tex.npz         hardware-filtered stop-map samples (border -1) at random points
   ref_<case>.npz  the reference's own kernels (oracle/_ref) on a few hundred seeds:
-                  pass-1 counts, streamline seeds, lengths and points
+                  pass-1 counts, streamline seeds, lengths and points (bootstrap:
+                  pass-1 counts only)
 
 Usage: python tests/golden/make_golden.py OUTDIR
 """
@@ -57,6 +58,10 @@ def main(out):
         inp = cases.inputs(name)
         ptt = cases.ptt_layout(name) if inp["case"]["model"] == "PTT" else None
         counts, lens, sidx, pts = ref.track(inp, s, ptt=ptt)
+        if lens is None:  # bootstrap: pass 1 only
+            np.savez_compressed(os.path.join(out, f"ref_{name}.npz"), seeds=s, counts=counts)
+            print(name, "pass-1 streamlines", int(counts.sum()))
+            continue
         np.savez_compressed(os.path.join(out, f"ref_{name}.npz"), seeds=s, counts=counts, lens=lens,
                             sidx=sidx, pts=pts)
         print(name, "streamlines", len(lens), "points", len(pts))
