@@ -64,7 +64,7 @@ EXPORTS = (
     "csl_create", "csl_destroy", "csl_propagate", "csl_propagate_device", "csl_counts",
     "csl_fetch", "csl_device_results", "csl_seed_peaks", "csl_get_direction",
     "csl_device_constants", "csl_philox_stream", "csl_last_error", "csl_version",
-    "csl_batch_timings",
+    "csl_batch_timings", "csl_track_noalloc",
 )
 
 
@@ -93,6 +93,7 @@ def load(path: str | None = None):
     lib.csl_get_direction.argtypes = [vp, _fp, _fp, ull_p, ull_p, ll, _fp, _fp, _ip, _ip]
     lib.csl_device_constants.argtypes = [vp, _fp, _fp]
     lib.csl_batch_timings.argtypes = [vp, _fp, _ip]
+    lib.csl_track_noalloc.argtypes = [vp, vp, ll, ll, C.c_int, vp, vp, vp, vp]
     lib.csl_philox_stream.argtypes = [C.c_ulonglong, C.c_ulonglong, C.c_ulonglong, ll,
                                       C.POINTER(C.c_uint)]
     lib.csl_last_error.argtypes = [vp, C.c_char_p, C.c_int]
@@ -230,6 +231,14 @@ class Handle:
         self._chk(self.lib.csl_get_direction(self.h, fptr(pts), fptr(ds), uptr(sq), uptr(of), n,
                                              fptr(fr), fptr(nd), iptr(ok), iptr(dr)))
         return nd, ok, dr, fr
+
+    def track_noalloc(self, seeds_ptr: int, n: int, rng_index_base: int, max_peaks: int,
+                      counts_ptr: int, lens_ptr: int, points_ptr: int, stream: int | None = None):
+        """Allocation-free tracking into caller-owned device buffers (see the C header)."""
+        self._chk(self.lib.csl_track_noalloc(self.h, C.c_void_p(seeds_ptr), int(n),
+                                             int(rng_index_base), int(max_peaks),
+                                             C.c_void_p(counts_ptr), C.c_void_p(lens_ptr),
+                                             C.c_void_p(points_ptr), stream))
 
     def timings(self):
         """(pass1_ms, gap_ms, pass2_ms, compact_ms), pass-2 runs of the last batch."""

@@ -85,6 +85,21 @@ struct csl_tracker {
     int pass2_runs = 0;
 };
 
+namespace csl {
+// internal accessors for the allocation-free entry point (noalloc.cu)
+int tracker_view(csl_tracker *t, DevParams *P, const int **partner, int *device) {
+    if (!t) return CSL_E_INVALID;
+    *P = t->P;
+    *partner = t->partner.p;
+    *device = t->device;
+    return CSL_OK;
+}
+int tracker_fail(csl_tracker *t, int code, const char *msg) {
+    if (t) t->err = msg;
+    return code;
+}
+}  // namespace csl
+
 static int fail(csl_tracker *t, int code, const char *fmt, ...) {
     char buf[512];
     va_list ap;

@@ -185,6 +185,29 @@ int csl_device_constants(csl_tracker *t, float *cos_max_angle, float *cos_min_se
 int csl_philox_stream(unsigned long long seed, unsigned long long subsequence,
                       unsigned long long offset, long long n, unsigned int *out);
 
+/*
+ * Allocation-free tracking, for callers that cannot call cudaMalloc while they
+ * track (device memory owned by a host framework's pool, no allocation after
+ * start-up).  No counterpart in the reference.  Runs a variant of the
+ * tracking kernel whose per-warp scratch is one static __device__ array of
+ * 9.5 MiB in the library (held by every GPU that loads it until exit); the
+ * call allocates nothing and only launches work on `stream`: results are
+ * ready when the stream reaches that point.  Inputs and outputs are DEVICE
+ * buffers owned by the caller:
+ *   seeds_dev  float32 [n,3]
+ *   counts_dev int32 [n]                      peaks per seed (all of them)
+ *   lens_dev   int32 [n*max_peaks]            length of slot s*max_peaks+k
+ *   points_dev float32 [n*max_peaks][2*max_sline_len][3]  slot s*max_peaks+k
+ * Only the first min(counts[s], max_peaks) slots of a seed are written; the
+ * streamlines equal csl_propagate's.  Limits (CSL_E_INVALID beyond them):
+ * 1 <= max_peaks <= 32, max_sline_len <= 501, at most 1024 sphere samples.
+ * The first call on a device looks up the scratch's device address (and
+ * loads the module): make it before any stream capture.  All calls share
+ * the scratch, so calls that overlap on the GPU race; serialise them.
+ */
+int csl_track_noalloc(csl_tracker *t, const float *seeds_dev, long long n, long long rng_index_base,
+                      int max_peaks, int *counts_dev, int *lens_dev, float *points_dev, void *stream);
+
 /* Last error message of the handle (or of the library when t is NULL). */
 int csl_last_error(const csl_tracker *t, char *buf, int buflen);
 
