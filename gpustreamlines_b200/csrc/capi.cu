@@ -314,6 +314,7 @@ int csl_create(const csl_params *params, const csl_inputs *inputs, int device, c
         P.sphere_symm = p.sphere_symm ? 1 : 0;
         P.max_sline_len = p.max_sline_len;
         P.nch = (p.model == PROB) ? (P.samplm_nr + 31) / 32 : 1;
+        P.vec4 = (p.model == PROB) && (P.samplm_nr % 4 == 0);
         P.step_frac = (p.model == PTT) ? p.step_frac : 1;
         P.step_size = p.step_size;
         P.max_angle = p.max_angle;

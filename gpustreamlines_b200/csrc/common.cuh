@@ -31,7 +31,8 @@ struct DevParams {
     int nvert, nedges, samplm_nr;
     int sphere_symm;
     int max_sline_len;
-    int nch;            // ceil(samplm_nr / 32) for PROB, ceil(dimt / 32) for BOOT
+    int nch;            // ceil(samplm_nr / 32) for PROB, 1 otherwise
+    int vec4;           // PROB: samplm_nr % 4 == 0 (16-byte aligned voxel rows)
     int step_frac;
     double step_size, max_angle, tc_threshold, relative_peak_thresh;
     double min_separation_angle, pmf_threshold;

@@ -22,6 +22,11 @@
 #include "ptt.cuh"
 #include "track.cuh"
 
+// resident 256-thread blocks per SM the probabilistic tracker is compiled for
+#ifndef CSL_PROB_MIN_BLOCKS
+#define CSL_PROB_MIN_BLOCKS 4
+#endif
+
 namespace csl {
 
 __host__ int smem_bytes(const DevParams &P, int warps, bool track) {
@@ -58,7 +63,7 @@ __global__ void __launch_bounds__(256) seed_peaks_kernel(DevParams P, const floa
 // pass 2: tracking
 
 template <int MODEL>
-__global__ void __launch_bounds__(256, MODEL == PROB ? 2 : 1) track_kernel(DevParams P, BatchArgs B, const int *partner,
+__global__ void __launch_bounds__(256, MODEL == PROB ? CSL_PROB_MIN_BLOCKS : 1) track_kernel(DevParams P, BatchArgs B, const int *partner,
                                                     const int *__restrict__ npeaks,
                                                     const short *__restrict__ peaks, int max_store,
                                                     const int *__restrict__ sl_off, int *out_len,

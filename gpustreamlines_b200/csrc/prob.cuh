@@ -10,6 +10,8 @@
 // vertices), and the table bits are produced on the device with the same dot
 // product expression, so the filter is bit-identical.
 #pragma once
+#include <cstring>
+
 #include "common.cuh"
 
 namespace csl {
@@ -22,44 +24,58 @@ struct DirState {
     int neg;
 };
 
-__device__ __forceinline__ int prob_get_direction(const DevParams &P, float3 pt, DirState dir,
-                                                  float *cdf_sh, Philox &rng, int lane,
-                                                  DirState *out, int *ndraws) {
-    Corners c;
-    if (!trilinear_setup(P, pt, c)) return 0;
-    const int len = P.samplm_nr;
-    const int nch = P.nch;
-    const float *rows[8];
-#pragma unroll
-    for (int q = 0; q < 8; q++) rows[q] = P.dataf + c.base[q];
+// Two fused multiply-adds with flush-to-zero, one instruction (Blackwell
+// packed FP32).  Each half rounds exactly as a scalar fma.rn.ftz.f32, the
+// form the reference's fast-math build uses for `acc += w * d`.
+__device__ __forceinline__ float2 ffma2_ftz(float2 a, float2 b, float2 c) {
+    unsigned long long ra, rb, rc, rd;
+    memcpy(&ra, &a, 8);
+    memcpy(&rb, &b, 8);
+    memcpy(&rc, &c, 8);
+    asm("fma.rn.ftz.f32x2 %0, %1, %2, %3;" : "=l"(rd) : "l"(ra), "l"(rb), "l"(rc));
+    float2 d;
+    memcpy(&d, &rd, 8);
+    return d;
+}
 
-    // gather (4 chunks of 32 vertices in flight per lane) + running max
+// Gather the trilinearly interpolated PMF into cdf_sh, return the lane's max.
+// Vector path: 128-bit loads (lane l owns float4 slots l, l+32, ...; every
+// voxel row is 16-byte aligned when V % 4 == 0) and packed FMAs; the per-
+// element order (corners in (i,j,k) order, acc = fma(w, d, acc)) is the
+// reference's.  Slot offsets are compile-time, so each load is one
+// instruction with an immediate offset.
+__device__ __forceinline__ float prob_gather(const DevParams &P, const Corners &c, float *cdf_sh,
+                                             int lane) {
+    const int len = P.samplm_nr;
     float m = -FLT_MAX;
-    int ch = 0;
-    for (; ch + 4 <= nch; ch += 4) {
-        float a[4];
+    if (P.vec4) {
+        constexpr int kNJ = 8;  // up to 1024 vertices
+        const int f4 = len >> 2;
+        const float4 *rows[8];
 #pragma unroll
-        for (int u = 0; u < 4; u++) {
-            const int t = (ch + u) * kWarp + lane;
-            float acc = 0.0f;
-            if (t < len) {
+        for (int q = 0; q < 8; q++) rows[q] = reinterpret_cast<const float4 *>(P.dataf + c.base[q]) + lane;
 #pragma unroll
-                for (int q = 0; q < 8; q++) acc += c.w[q] * __ldg(rows[q] + t);
+        for (int j = 0; j < kNJ; j++) {
+            if (lane + 32 * j < f4) {
+                float4 d[8];
+#pragma unroll
+                for (int q = 0; q < 8; q++) d[q] = __ldg(rows[q] + 32 * j);
+                float2 lo = make_float2(0.0f, 0.0f), hi = make_float2(0.0f, 0.0f);
+#pragma unroll
+                for (int q = 0; q < 8; q++) {
+                    const float2 ww = make_float2(c.w[q], c.w[q]);
+                    lo = ffma2_ftz(make_float2(d[q].x, d[q].y), ww, lo);
+                    hi = ffma2_ftz(make_float2(d[q].z, d[q].w), ww, hi);
+                }
+                reinterpret_cast<float4 *>(cdf_sh)[lane + 32 * j] = make_float4(lo.x, lo.y, hi.x, hi.y);
+                m = fmax_ref(fmax_ref(fmax_ref(fmax_ref(m, lo.x), lo.y), hi.x), hi.y);
             }
-            a[u] = acc;
         }
+    } else {
+        const float *rows[8];
 #pragma unroll
-        for (int u = 0; u < 4; u++) {
-            const int t = (ch + u) * kWarp + lane;
-            if (t < len) {
-                cdf_sh[t] = a[u];
-                m = fmax_ref(m, a[u]);
-            }
-        }
-    }
-    for (; ch < nch; ch++) {
-        const int t = ch * kWarp + lane;
-        if (t < len) {
+        for (int q = 0; q < 8; q++) rows[q] = P.dataf + c.base[q];
+        for (int t = lane; t < len; t += kWarp) {
             float acc = 0.0f;
 #pragma unroll
             for (int q = 0; q < 8; q++) acc += c.w[q] * __ldg(rows[q] + t);
@@ -67,23 +83,36 @@ __device__ __forceinline__ int prob_get_direction(const DevParams &P, float3 pt,
             m = fmax_ref(m, acc);
         }
     }
+    return m;
+}
+
+__device__ __forceinline__ int prob_get_direction(const DevParams &P, float3 pt, DirState dir,
+                                                  float *cdf_sh, Philox &rng, int lane,
+                                                  DirState *out, int *ndraws) {
+    Corners c;
+    if (!trilinear_setup(P, pt, c)) return 0;
+    const int len = P.samplm_nr;
+    const int nch = P.nch;
+    float m = prob_gather(P, c, cdf_sh, lane);
     m = warp_max_ref(m);
     const float thr = (float)(P.pmf_threshold * (double)m);
     __syncwarp();
 
-    // threshold + cone filter + reference-order scan, chunk by chunk
+    // threshold + cone filter + reference-order scan, chunk by chunk.  A chunk
+    // whose 32 values are all zero scans to the carry in every position (each
+    // addition adds an exact zero), so it is written without the shuffle tree.
     const uint32_t *row = (dir.vtx >= 0)
                               ? P.cone_mask + ((size_t)dir.neg * P.nvert + dir.vtx) * nch
                               : nullptr;
+    const uint32_t my_word = (row && lane < nch) ? __ldg(row + lane) : 0u;
     const float cos_similarity = P.cos_max_angle;
     float carry = 0.0f;
-    for (ch = 0; ch < nch; ch++) {
+    for (int ch = 0; ch < nch; ch++) {
         const int t = ch * kWarp + lane;
         const bool valid = t < len;
-        float x = valid ? cdf_sh[t] : 0.0f;
         bool keep;
         if (row) {
-            keep = (__ldg(row + ch) >> lane) & 1u;
+            keep = (__shfl_sync(FULL, my_word, ch) >> lane) & 1u;
         } else {
             keep = true;
             if (valid) {
@@ -93,7 +122,15 @@ __device__ __forceinline__ int prob_get_direction(const DevParams &P, float3 pt,
                 keep = !(dot < cos_similarity);
             }
         }
-        if (x < thr || !keep) x = 0.0f;
+        float x = 0.0f;
+        if (keep && valid) {
+            x = cdf_sh[t];
+            if (x < thr) x = 0.0f;
+        }
+        if (__ballot_sync(FULL, x != 0.0f) == 0u) {
+            if (valid) cdf_sh[t] = carry;
+            continue;
+        }
         if (lane == 0 && ch != 0) x = x + carry;
 #pragma unroll
         for (int i = 1; i < kWarp; i <<= 1) {

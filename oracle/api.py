@@ -213,18 +213,18 @@ class Reference:
         L.ref_track.restype = C.c_longlong
         L.ref_track.argtypes = [_fp, C.c_int, _fp, _fp, _fp, _ip, _fp, _fp, _fp, _fp, _fp, _ip,
                                 C.c_float, C.c_int, _fp, C.c_int, C.c_int, C.c_int, _fp, C.c_int, _ip,
-                                _fp, C.c_int, _ip, _ip, _fp]
+                                _fp, C.c_int, _ip, _ip, _fp, _fp]
         self.L = L
         self.name = case_name
 
-    def track(self, inp: dict, seeds, cap=None, ptt=None):
+    def track(self, inp: dict, seeds, cap=None, ptt=None, points=True):
         seeds = np.ascontiguousarray(seeds, dtype=np.float32)
         n = len(seeds)
         counts = np.zeros(n, dtype=np.int32)
         cap = cap if cap is not None else 12 * n + 16
         sl_seed = np.zeros(cap, dtype=np.int32)
         sl_len = np.zeros(cap, dtype=np.int32)
-        slines = np.zeros((cap, 2 * 501 * 3), dtype=np.float32)
+        slines = np.zeros((cap if points else 1, 2 * 501 * 3), dtype=np.float32)
         boot = "H" in inp
         args = [_f(seeds), n, _f(inp["dataf"]) if ptt is None else None, _f(inp["stop_map"]),
                 _f(inp["vertices"]), _i(inp["edges"])]
@@ -239,15 +239,20 @@ class Reference:
             args += [_f(t), t.shape[2], t.shape[1], t.shape[0], _f(ptt["lut"]), int(ptt["res"])]
         else:
             args += [None, 0, 0, 0, None, 0]
-        args += [_i(counts), None, cap, _i(sl_seed), _i(sl_len), slines.ctypes.data_as(_fp)]
+        ms = np.zeros(2, dtype=np.float32)
+        args += [_i(counts), None, cap, _i(sl_seed), _i(sl_len),
+                 slines.ctypes.data_as(_fp) if points else None, ms.ctypes.data_as(_fp)]
         nsl = self.L.ref_track(*args)
+        self.last_ms = (float(ms[0]), float(ms[1]))
         if nsl < 0:
             raise RuntimeError(f"reference kernels failed ({nsl})")
         if boot:  # pass 1 only: the reference's bootstrap pass 2 is not launched
             return counts, None, None, None
         if nsl > cap:
-            return self.track(inp, seeds, cap=int(nsl) + 16, ptt=ptt)
+            return self.track(inp, seeds, cap=int(nsl) + 16, ptt=ptt, points=points)
         sl_seed, sl_len = sl_seed[:nsl], sl_len[:nsl]
+        if not points:
+            return counts, sl_len, sl_seed, None
         flat = np.concatenate([slines[j, :3 * sl_len[j]].reshape(-1, 3) for j in range(nsl)]) if nsl \
             else np.zeros((0, 3), np.float32)
         return counts, sl_len, sl_seed, flat

@@ -73,7 +73,8 @@ extern "C" const char *ref_config(void) {
 //   counts[n]                       pass-1 peak counts (slineOutOff before the scan)
 //   dirs[n * SAMPLM_NR * 3]         pass-1 directions (may be NULL)
 //   sl_seed[cap], sl_len[cap]       slineSeed / slineLen
-//   slines[cap * 2*MAX_SLINE_LEN*3] padded streamline buffer
+//   slines[cap * 2*MAX_SLINE_LEN*3] padded streamline buffer (may be NULL: not copied)
+//   ms_out[2]                       pass-1 / pass-2 kernel times, CUDA events (may be NULL)
 // Returns the number of streamlines (or a negative error); when it exceeds
 // `cap` only counts/dirs are filled.
 extern "C" long long ref_track(const float *seeds, int n, const float *dataf, const float *stop_map,
@@ -82,8 +83,10 @@ extern "C" long long ref_track(const float *seeds, int n, const float *dataf, co
                                const int *b0s, float min_signal, int delta_nr,
                                const float *ptt_tiled, int tw, int th, int td, const float *ptt_lut,
                                int lut_res, int *counts, float *dirs, int cap, int *sl_seed,
-                               int *sl_len, float *slines) {
+                               int *sl_len, float *slines, float *ms_out) {
     if (n <= 0) return 0;
+    cudaEvent_t ev[4];
+    for (auto &e : ev) cudaEventCreate(&e);
     const int block_y = THR_X_BL / THR_X_SL;
     dim3 block(THR_X_SL, block_y, 1);
     dim3 grid((n + block_y - 1) / block_y, 1, 1);
@@ -129,6 +132,7 @@ extern "C" long long ref_track(const float *seeds, int n, const float *dataf, co
 #endif
 
     // pass 1
+    cudaEventRecord(ev[0]);
 #if REF_MODEL == 2
     getNumStreamlinesProb_k<THR_X_SL, THR_X_BL / THR_X_SL, float, float3>
         <<<grid, block>>>(n, seeds_d, dataf_d, (float3 *)verts_d, edges_d, shdir_d, offs_d);
@@ -143,7 +147,9 @@ extern "C" long long ref_track(const float *seeds, int n, const float *dataf, co
         smp_d, (float3 *)verts_d, edges_d, shdir_d, offs_d);
 #endif
     REF_CK(cudaGetLastError());
+    cudaEventRecord(ev[1]);
     REF_CK(cudaDeviceSynchronize());
+    if (ms_out) cudaEventElapsedTime(&ms_out[0], ev[0], ev[1]);
     std::vector<int> off(n + 1);
     REF_CK(cudaMemcpy(off.data(), offs_d, sizeof(int) * n, cudaMemcpyDeviceToHost));
     for (int s = 0; s < n; s++) counts[s] = off[s];
@@ -176,6 +182,7 @@ extern "C" long long ref_track(const float *seeds, int n, const float *dataf, co
         int *len_d = dev_copy<int>(nullptr, nsl);
         float3 *sl_d = (float3 *)dev_copy<float>(nullptr, (size_t)nsl * 2 * MAX_SLINE_LEN * 3);
         REF_CK(cudaMemset(seed_d, 0xff, sizeof(int) * nsl));
+        cudaEventRecord(ev[2]);
 #if REF_MODEL == 2
         genStreamlinesMergeProb_k<THR_X_SL, THR_X_BL / THR_X_SL, PROB, const float *__restrict__, float,
                                   float3><<<grid, block>>>(0, n, seeds_d, dataf_d, stop_tex_d, verts_d,
@@ -188,15 +195,19 @@ extern "C" long long ref_track(const float *seeds, int n, const float *dataf, co
                               seed_d, len_d, sl_d);
 #endif
         REF_CK(cudaGetLastError());
+        cudaEventRecord(ev[3]);
         REF_CK(cudaDeviceSynchronize());
+        if (ms_out) cudaEventElapsedTime(&ms_out[1], ev[2], ev[3]);
         REF_CK(cudaMemcpy(sl_seed, seed_d, sizeof(int) * nsl, cudaMemcpyDeviceToHost));
         REF_CK(cudaMemcpy(sl_len, len_d, sizeof(int) * nsl, cudaMemcpyDeviceToHost));
-        REF_CK(cudaMemcpy(slines, sl_d, (size_t)nsl * 2 * MAX_SLINE_LEN * 12, cudaMemcpyDeviceToHost));
+        if (slines)
+            REF_CK(cudaMemcpy(slines, sl_d, (size_t)nsl * 2 * MAX_SLINE_LEN * 12, cudaMemcpyDeviceToHost));
         cudaFree(seed_d);
         cudaFree(len_d);
         cudaFree(sl_d);
     }
 done:
+    for (auto &e : ev) cudaEventDestroy(e);
     cudaFree(seeds_d); cudaFree(verts_d); cudaFree(edges_d); cudaFree(offs_d); cudaFree(shdir_d);
     cudaFree(stop_tex_d); cudaDestroyTextureObject(stop_tex); cudaFreeArray(stop_arr);
     if (dataf_d) cudaFree(dataf_d);
