@@ -31,7 +31,7 @@ class CslParams(C.Structure):
         ("model", C.c_int),
         ("dimx", C.c_int), ("dimy", C.c_int), ("dimz", C.c_int), ("dimt", C.c_int),
         ("nvertices", C.c_int), ("nedges", C.c_int), ("samplm_nr", C.c_int),
-        ("sphere_symm", C.c_int), ("max_sline_len", C.c_int), ("_pad0", C.c_int),
+        ("sphere_symm", C.c_int), ("max_sline_len", C.c_int), ("seed_order", C.c_int),
         ("step_size", C.c_double), ("max_angle", C.c_double), ("tc_threshold", C.c_double),
         ("relative_peak_thresh", C.c_double), ("min_separation_angle", C.c_double),
         ("pmf_threshold", C.c_double), ("rng_seed", C.c_ulonglong),

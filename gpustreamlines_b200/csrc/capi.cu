@@ -63,7 +63,7 @@ struct csl_tracker {
     // inputs
     DevBuf<float> dataf, verts, H, R, delta_b, delta_q, sampling;
     DevBuf<int> edges, b0s, partner;
-    DevBuf<uint32_t> cone;
+    DevBuf<uint32_t> cone, cone_t;
     cudaArray_t stop_arr = nullptr, odf_arr = nullptr, lut_arr = nullptr;
     cudaTextureObject_t stop_tex = 0, odf_tex = 0, lut_tex = 0;
     DevBuf<float> consts;
@@ -74,7 +74,9 @@ struct csl_tracker {
     DevBuf<long long> out_src, pt_off;
     DevBuf<unsigned long long> pool_count;
     DevBuf<float> pool, scratch, points;
-    DevBuf<unsigned char> scan_tmp;
+    DevBuf<unsigned char> scan_tmp, sort_tmp;
+    DevBuf<uint32_t> mkeys, mkeys_sorted;
+    DevBuf<int> mvals, perm, blk_next, blk_end;
     long long *host_stage = nullptr;  // pinned 16-byte staging for the two totals
     long long last_n = -1, nsl = 0, npts = 0;
     int ok_batch = 0;
@@ -213,6 +215,7 @@ static void release_all(csl_tracker *t) {
                          &t->out_len, &t->out_seed, &t->queue, &t->status};
     for (auto *b : ib) b->release();
     t->cone.release();
+    t->cone_t.release();
     t->peaks.release();
     t->out_src.release();
     t->pt_off.release();
@@ -235,6 +238,7 @@ static int validate(const csl_params *p, const csl_inputs *in, csl_tracker *t) {
     if (p->nvertices <= 0 || p->nedges <= 0) return fail(t, CSL_E_INVALID, "empty sphere");
     if (p->nvertices > 32767) return fail(t, CSL_E_INVALID, "at most 32767 sphere vertices");
     if (p->max_sline_len < 2) return fail(t, CSL_E_INVALID, "max_sline_len must be >= 2");
+    if (p->seed_order != 0 && p->seed_order != 1) return fail(t, CSL_E_INVALID, "seed_order must be 0 or 1");
     if (!in->stop_map || !in->vertices || !in->edges)
         return fail(t, CSL_E_INVALID, "stop_map, vertices and edges are required");
     const bool boot = p->model == CSL_MODEL_OPDT || p->model == CSL_MODEL_CSA;
@@ -376,8 +380,10 @@ int csl_create(const csl_params *params, const csl_inputs *inputs, int device, c
         }
         if (p.model == PROB) {
             CK(t->cone.ensure((size_t)2 * P.nvert * P.nch));
+            CK(t->cone_t.ensure((size_t)2 * P.nvert * kWarp));
             P.cone_mask = t->cone.p;
-            CK(launch_cone_mask(P, t->cone.p, t->own_stream));
+            P.cone_mask_t = t->cone_t.p;
+            CK(launch_cone_mask(P, t->cone.p, t->cone_t.p, t->own_stream));
         }
         if (p.model == PTT) {
             r = make_texture3d(t, inputs->ptt_odf_tiled, p.tile_nx * p.dimx, p.tile_ny * p.dimy,
@@ -481,6 +487,18 @@ static int run_batch(csl_tracker *t, const float *seeds_dev, long long n, long l
     const int grid2 = (int)std::max<long long>(
         1, std::min<long long>((long long)t->nsm * t->blocks_per_sm, (warps_needed + wpb - 1) / wpb));
     CK(t->scratch.ensure((size_t)grid2 * wpb * scratch_floats_per_warp(P)));
+    if (t->hp.seed_order == 1) {
+        size_t sb = 0;
+        CK(spatial_order(nullptr, ni, grid2, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr,
+                         nullptr, &sb, st));
+        CK(t->sort_tmp.ensure(sb));
+        CK(t->mkeys.ensure(ni));
+        CK(t->mkeys_sorted.ensure(ni));
+        CK(t->mvals.ensure(ni));
+        CK(t->perm.ensure(ni));
+        CK(t->blk_next.ensure(grid2));
+        CK(t->blk_end.ensure(grid2));
+    }
     unsigned long long want = std::max<unsigned long long>(t->pool.cap / 3, (unsigned long long)nsl * 96ull);
     for (int attempt = 0; attempt < 2; attempt++) {
         CK(t->pool.ensure(want * 3));
@@ -494,6 +512,14 @@ static int run_batch(csl_tracker *t, const float *seeds_dev, long long n, long l
         B.pool_cap = t->pool.cap / 3;
         B.scratch = t->scratch.p;
         B.status = t->status.p;
+        if (t->hp.seed_order == 1) {
+            size_t sb = t->sort_tmp.cap;
+            CK(spatial_order(seeds_dev, ni, grid2, t->mkeys.p, t->mkeys_sorted.p, t->mvals.p, t->perm.p,
+                             t->blk_next.p, t->blk_end.p, t->sort_tmp.p, &sb, st));
+            B.perm = t->perm.p;
+            B.blk_next = t->blk_next.p;
+            B.blk_end = t->blk_end.p;
+        }
         CK(cudaMemsetAsync(t->queue.p, 0, sizeof(int), st));
         CK(cudaMemsetAsync(t->status.p, 0, sizeof(int), st));
         CK(cudaMemsetAsync(t->pool_count.p, 0, sizeof(unsigned long long), st));

@@ -43,7 +43,8 @@ struct DevParams {
     const float *__restrict__ verts;     // [V,3]
     const int2 *__restrict__ edges;      // [E]
     cudaTextureObject_t stop_tex;        // stop map, border -1, linear filter
-    const uint32_t *__restrict__ cone_mask;  // PROB: [2][V][nch] keep bits
+    const uint32_t *__restrict__ cone_mask;    // PROB: [2][V][nch] keep bits
+    const uint32_t *__restrict__ cone_mask_t;  // PROB: [2][V][32] the same bits, per lane
     // bootstrap
     float min_signal;
     int delta_nr, hr_side;
@@ -66,7 +67,10 @@ struct BatchArgs {
     const float *__restrict__ seeds;    // [n,3]
     int nseeds;
     long long rng_index_base;
-    int *queue;                         // atomic seed counter
+    int *queue;                         // atomic seed counter (input order)
+    const int *__restrict__ perm;       // spatial order: position -> seed (or nullptr)
+    int *blk_next;                      // per-block next position in `perm`
+    const int *__restrict__ blk_end;    // per-block end position
     unsigned long long *pool_count;     // atomic, in points
     float *pool;                        // [pool_cap,3]
     unsigned long long pool_cap;

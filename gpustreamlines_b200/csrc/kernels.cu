@@ -12,6 +12,7 @@
 // genStreamlinesMerge*_k), reserves space in the pool with one atomicAdd
 // and copies the streamline there.  Uneven streamline lengths therefore
 // never idle a warp while work remains.
+#include <cub/device/device_radix_sort.cuh>
 #include <cub/device/device_scan.cuh>
 #include <cuda_runtime.h>
 
@@ -62,6 +63,53 @@ __global__ void __launch_bounds__(256) seed_peaks_kernel(DevParams P, const floa
 // ---------------------------------------------------------------------------
 // pass 2: tracking
 
+// Next seed for the calling warp (lane 0).  Input order: one global counter.
+// Spatial order: the seeds are sorted by the Morton code of their voxel and
+// each block owns a contiguous range of that order, so the warps of a block
+// track neighbouring seeds at the same time and share voxel rows in L1; a
+// block whose range is exhausted takes positions from the following blocks'
+// ranges.  Every position is claimed exactly once; results do not depend on
+// the order.
+__device__ __forceinline__ int next_seed(const BatchArgs &B) {
+    if (!B.perm) return atomicAdd(B.queue, 1);
+    const int nb = gridDim.x;
+    for (int k = 0; k < nb; k++) {
+        const int b = (blockIdx.x + k) % nb;
+        const int p = atomicAdd(B.blk_next + b, 1);
+        if (p < B.blk_end[b]) return B.perm[p];
+    }
+    return B.nseeds;
+}
+
+// 30-bit Morton code of each seed's voxel (10 bits per axis)
+__device__ __forceinline__ uint32_t spread3(uint32_t v) {
+    v &= 0x3ffu;
+    v = (v | (v << 16)) & 0x030000ffu;
+    v = (v | (v << 8)) & 0x0300f00fu;
+    v = (v | (v << 4)) & 0x030c30c3u;
+    v = (v | (v << 2)) & 0x09249249u;
+    return v;
+}
+
+__global__ void morton_kernel(const float *__restrict__ seeds, int n, uint32_t *keys, int *vals) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    uint32_t c[3];
+    for (int a = 0; a < 3; a++) {
+        const float f = floorf(seeds[3 * i + a] + 0.5f);
+        c[a] = (f != f || f < 0.0f) ? 0u : (f > 1023.0f ? 1023u : (uint32_t)f);
+    }
+    keys[i] = spread3(c[0]) | (spread3(c[1]) << 1) | (spread3(c[2]) << 2);
+    vals[i] = i;
+}
+
+__global__ void block_ranges_kernel(int n, int nblocks, int *next, int *end) {
+    const int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= nblocks) return;
+    next[b] = (int)((long long)n * b / nblocks);
+    end[b] = (int)((long long)n * (b + 1) / nblocks);
+}
+
 template <int MODEL>
 __global__ void __launch_bounds__(256, MODEL == PROB ? CSL_PROB_MIN_BLOCKS : 1) track_kernel(DevParams P, BatchArgs B, const int *partner,
                                                     const int *__restrict__ npeaks,
@@ -81,7 +129,7 @@ __global__ void __launch_bounds__(256, MODEL == PROB ? CSL_PROB_MIN_BLOCKS : 1) 
 
     for (;;) {
         int s = 0;
-        if (lane == 0) s = atomicAdd(B.queue, 1);
+        if (lane == 0) s = next_seed(B);
         s = __shfl_sync(FULL, s, 0);
         if (s >= B.nseeds) break;
         const int np = npeaks[s];
@@ -97,6 +145,7 @@ __global__ void __launch_bounds__(256, MODEL == PROB ? CSL_PROB_MIN_BLOCKS : 1) 
         }
         __syncwarp();
         typename RngOf<MODEL>::T rng;
+        if constexpr (MODEL == PROB) rng.st = W.rng;
         rng.init(P.rng_seed, gid + 1, 0);
         const int base = sl_off[s];
         {
@@ -197,6 +246,17 @@ __global__ void cone_mask_kernel(DevParams P, uint32_t *mask) {
     }
 }
 
+// the same keep bits transposed per lane: word (row, l) bit ch = vertex 32*ch+l
+__global__ void cone_mask_t_kernel(DevParams P, const uint32_t *mask, uint32_t *mask_t) {
+    const int lane = threadIdx.x & 31;
+    const int row = blockIdx.x * (blockDim.x / kWarp) + threadIdx.x / kWarp;
+    if (row >= 2 * P.nvert) return;
+    uint32_t bits = 0u;
+    for (int ch = 0; ch < P.nch; ch++)
+        bits |= ((mask[(size_t)row * P.nch + ch] >> lane) & 1u) << ch;
+    mask_t[(size_t)row * kWarp + lane] = bits;
+}
+
 __global__ void device_cos_kernel(float a, float b, float *out) {
     out[0] = __cosf(a);
     out[1] = __cosf(b);
@@ -229,6 +289,7 @@ __global__ void get_direction_kernel(DevParams P, const int *partner, const floa
     const float3 pt = make_float3(pts[3 * q], pts[3 * q + 1], pts[3 * q + 2]);
     DirState d{make_float3(dirs[3 * q], dirs[3 * q + 1], dirs[3 * q + 2]), -1, 0};
     typename RngOf<MODEL>::T rng;
+    if constexpr (MODEL == PROB) rng.st = W.rng;
     rng.init(P.rng_seed, subseq[q] + lane, offs[q]);
     DirState nd;
     nd.d = d.d;
@@ -338,9 +399,12 @@ cudaError_t launch_gather(const float *pool, const long long *src, const int *le
     return cudaGetLastError();
 }
 
-cudaError_t launch_cone_mask(const DevParams &P, uint32_t *mask, cudaStream_t st) {
+cudaError_t launch_cone_mask(const DevParams &P, uint32_t *mask, uint32_t *mask_t, cudaStream_t st) {
     const int rows = 2 * P.nvert;
     cone_mask_kernel<<<(rows + 7) / 8, 256, 0, st>>>(P, mask);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    cone_mask_t_kernel<<<(rows + 7) / 8, 256, 0, st>>>(P, mask, mask_t);
     return cudaGetLastError();
 }
 
@@ -357,6 +421,22 @@ cudaError_t launch_philox_stream(unsigned long long seed, unsigned long long sub
 }
 
 // temporary storage for an n-element exclusive scan (either output type)
+cudaError_t spatial_order(const float *seeds, int n, int nblocks, uint32_t *keys, uint32_t *keys_sorted,
+                          int *vals, int *perm, int *blk_next, int *blk_end, void *tmp,
+                          size_t *tmp_bytes, cudaStream_t st) {
+    if (!tmp) {
+        return cub::DeviceRadixSort::SortPairs(nullptr, *tmp_bytes, keys, keys_sorted, vals, perm, n, 0,
+                                               30, st);
+    }
+    morton_kernel<<<(n + 255) / 256, 256, 0, st>>>(seeds, n, keys, vals);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    e = cub::DeviceRadixSort::SortPairs(tmp, *tmp_bytes, keys, keys_sorted, vals, perm, n, 0, 30, st);
+    if (e != cudaSuccess) return e;
+    block_ranges_kernel<<<(nblocks + 255) / 256, 256, 0, st>>>(n, nblocks, blk_next, blk_end);
+    return cudaGetLastError();
+}
+
 cudaError_t scan_temp_bytes(int n, size_t *bytes) {
     size_t a = 0, b = 0;
     cudaError_t e = cub::DeviceScan::ExclusiveSum(nullptr, a, (const int *)nullptr, (int *)nullptr, n);

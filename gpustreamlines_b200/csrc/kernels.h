@@ -32,12 +32,17 @@ cudaError_t launch_get_direction(const DevParams &P, const int *partner, const f
                                  float *out_dirs, int *out_ok, int *out_draws, cudaStream_t st);
 cudaError_t launch_gather(const float *pool, const long long *src, const int *len,
                           const long long *pt_off, int nsl, float *out, int grid, cudaStream_t st);
-cudaError_t launch_cone_mask(const DevParams &P, uint32_t *mask, cudaStream_t st);
+cudaError_t launch_cone_mask(const DevParams &P, uint32_t *mask, uint32_t *mask_t, cudaStream_t st);
 cudaError_t launch_device_cos(float a, float b, float *out, cudaStream_t st);
 cudaError_t launch_philox_stream(unsigned long long seed, unsigned long long subseq,
                                  unsigned long long offset, long long n, unsigned *out,
                                  cudaStream_t st);
 cudaError_t scan_temp_bytes(int n, size_t *bytes);
+// Morton-sort the seeds (perm = position -> seed) and split the order into
+// per-block ranges; with tmp == nullptr only reports the sort's temp size.
+cudaError_t spatial_order(const float *seeds, int n, int nblocks, uint32_t *keys, uint32_t *keys_sorted,
+                          int *vals, int *perm, int *blk_next, int *blk_end, void *tmp,
+                          size_t *tmp_bytes, cudaStream_t st);
 cudaError_t exclusive_scan_i32(void *tmp, size_t tmp_bytes, const int *in, int *out, int n,
                                cudaStream_t st);
 cudaError_t exclusive_scan_i64(void *tmp, size_t tmp_bytes, const int *in, long long *out, int n,

@@ -76,6 +76,7 @@ __global__ void __launch_bounds__(kNoallocWarpsPerBlock * 32)
         if (lane == 0) counts_out[s] = np;
         __syncwarp();
         typename RngOf<MODEL>::T rng;
+        if constexpr (MODEL == PROB) rng.st = W.rng;
         rng.init(P.rng_seed, gid + 1, 0);
         const int ntrack = np < max_peaks ? np : max_peaks;
         for (int k = 0; k < ntrack; k++) {

@@ -89,4 +89,15 @@ struct Philox {
     }
 };
 
+// Generator whose state lives in shared memory and is advanced by lane 0
+// only (the probabilistic getter draws one uniform per step on lane 0).
+struct PhiloxShared {
+    Philox *st;
+    __device__ __forceinline__ void init(uint64_t seed, uint64_t subsequence, uint64_t offset) {
+        if ((threadIdx.x & 31) == 0) st->init(seed, subsequence, offset);
+        __syncwarp();
+    }
+    __device__ __forceinline__ float uniform() { return st->uniform(); }
+};
+
 }  // namespace csl

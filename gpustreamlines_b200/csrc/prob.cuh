@@ -4,7 +4,8 @@
 // reference-order inclusive scan, one Philox uniform drawn by lane 0, the
 // reference's bisection + ballot search, and the hemisphere flip.
 //
-// The cone filter reads a precomputed keep-bit table instead of evaluating
+// The cone filter reads a precomputed keep-bit table (one 32-bit word per
+// lane and step, bit c for vertex 32c + lane) instead of evaluating
 // 3 * V multiply-adds per step: along a streamline the incoming direction is
 // always +/- a sphere vertex (pass-1 peaks and every sampled step are
 // vertices), and the table bits are produced on the device with the same dot
@@ -86,14 +87,11 @@ __device__ __forceinline__ float prob_gather(const DevParams &P, const Corners &
     return m;
 }
 
-__device__ __forceinline__ int prob_get_direction(const DevParams &P, float3 pt, DirState dir,
-                                                  float *cdf_sh, Philox &rng, int lane,
-                                                  DirState *out, int *ndraws) {
-    Corners c;
-    if (!trilinear_setup(P, pt, c)) return 0;
+__device__ __forceinline__ int prob_finish(const DevParams &P, float m, DirState dir,
+                                           float *cdf_sh, PhiloxShared &rng, int lane,
+                                           DirState *out, int *ndraws) {
     const int len = P.samplm_nr;
     const int nch = P.nch;
-    float m = prob_gather(P, c, cdf_sh, lane);
     m = warp_max_ref(m);
     const float thr = (float)(P.pmf_threshold * (double)m);
     __syncwarp();
@@ -104,7 +102,9 @@ __device__ __forceinline__ int prob_get_direction(const DevParams &P, float3 pt,
     const uint32_t *row = (dir.vtx >= 0)
                               ? P.cone_mask + ((size_t)dir.neg * P.nvert + dir.vtx) * nch
                               : nullptr;
-    const uint32_t my_word = (row && lane < nch) ? __ldg(row + lane) : 0u;
+    // keep bits of this lane, one coalesced word: bit ch <=> vertex 32*ch + lane
+    const uint32_t kbits_t = (dir.vtx >= 0)
+        ? __ldg(P.cone_mask_t + ((size_t)dir.neg * P.nvert + dir.vtx) * kWarp + lane) : 0u;
     const float cos_similarity = P.cos_max_angle;
     float carry = 0.0f;
     for (int ch = 0; ch < nch; ch++) {
@@ -112,7 +112,7 @@ __device__ __forceinline__ int prob_get_direction(const DevParams &P, float3 pt,
         const bool valid = t < len;
         bool keep;
         if (row) {
-            keep = (__shfl_sync(FULL, my_word, ch) >> lane) & 1u;
+            keep = (kbits_t >> ch) & 1u;
         } else {
             keep = true;
             if (valid) {
@@ -174,6 +174,60 @@ __device__ __forceinline__ int prob_get_direction(const DevParams &P, float3 pt,
     }
     out->vtx = ind;
     return 1;
+}
+
+__device__ __forceinline__ int prob_get_direction(const DevParams &P, float3 pt, DirState dir,
+                                                  float *cdf_sh, PhiloxShared &rng, int lane,
+                                                  DirState *out, int *ndraws) {
+    Corners c;
+    if (!trilinear_setup(P, pt, c)) return 0;
+    const float m = prob_gather(P, c, cdf_sh, lane);
+    return prob_finish(P, m, dir, cdf_sh, rng, lane, out, ndraws);
+}
+
+// One tracking direction of the probabilistic getter (tracker_d,
+// generate_streamlines_cuda.cu:283-421) with the stop-map check of step i
+// overlapped with the PMF gather of step i + 1: the texture fetch is issued,
+// the next gather's loads go out, and only then is the check evaluated.  A
+// stop discards the gathered values (no random number has been drawn yet),
+// so points, counts and RNG consumption are exactly the sequential ones.
+__device__ __forceinline__ int prob_track(const DevParams &P, PhiloxShared &rng, float3 seed, DirState dir,
+                                          float *out, float *cdf_sh, int lane) {
+    float3 pt = seed;
+    if (lane == 0) { out[0] = pt.x; out[1] = pt.y; out[2] = pt.z; }
+    __syncwarp();
+    const int imax = P.max_sline_len;
+    float sval = 0.0f;
+    bool pending = false;
+    int i = 1;
+    for (;;) {
+        if (i >= imax) {
+            if (pending && !((double)sval > P.tc_threshold)) i = i - 1;
+            break;
+        }
+        Corners c;
+        const bool inb = trilinear_setup(P, pt, c);
+        float m = -FLT_MAX;
+        if (inb) m = prob_gather(P, c, cdf_sh, lane);
+        if (pending) {
+            pending = false;
+            // check_point_d: -1 (outside) and values <= the threshold both stop
+            if (!((double)sval > P.tc_threshold)) { i = i - 1; break; }
+        }
+        if (!inb) break;
+        DirState nd;
+        if (!prob_finish(P, m, dir, cdf_sh, rng, lane, &nd, nullptr)) break;
+        dir = nd;
+        pt.x = (float)fma((double)dir.d.x, P.step_size, (double)pt.x);
+        pt.y = (float)fma((double)dir.d.y, P.step_size, (double)pt.y);
+        pt.z = (float)fma((double)dir.d.z, P.step_size, (double)pt.z);
+        if (lane == 0) { out[3 * i] = pt.x; out[3 * i + 1] = pt.y; out[3 * i + 2] = pt.z; }
+        sval = tex3D<float>(P.stop_tex, pt.z, pt.y, pt.x);
+        pending = true;
+        i++;
+    }
+    __syncwarp();
+    return i;
 }
 
 // Pass-1 peaks at a seed (getNumStreamlinesProb_k, generate_streamlines_cuda.cu:427-462).

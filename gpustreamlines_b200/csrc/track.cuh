@@ -21,6 +21,7 @@ struct WarpBufs {
     float *msk;     // BOOT [n32t]
     float *r;       // BOOT [rh]
     float *h;       // BOOT [rh]
+    Philox *rng;    // PROB: lane 0's generator state
     float *frame;   // PTT [18]
     float *face;    // PTT [32]
     float *vpdf;    // PTT [32]
@@ -39,6 +40,7 @@ __host__ __device__ inline int warp_smem_floats(const DevParams &P, bool track) 
     }
     int f = track ? nr : 2 * nr;
     if (P.model == PTT) f += 18 + 32 + 32;
+    if (P.model == PROB) f += 16;
     return f;
 }
 
@@ -60,6 +62,7 @@ __device__ inline WarpBufs carve(const DevParams &P, float *base, int warp, bool
         b.odf = p;
         const int f = track ? nr : 2 * nr;
         b.ind = track ? global_ind : reinterpret_cast<int *>(p + nr);
+        if (P.model == PROB) b.rng = reinterpret_cast<Philox *>(p + f);
         if (P.model == PTT) {
             b.frame = p + f;
             b.face = b.frame + 18;
@@ -98,6 +101,10 @@ struct RngOf {
     using T = Philox;
 };
 template <>
+struct RngOf<PROB> {
+    using T = PhiloxShared;
+};
+template <>
 struct RngOf<PTT> {
     using T = PhiloxN;
 };
@@ -113,6 +120,7 @@ template <int MODEL>
 __device__ __forceinline__ int track_one(const DevParams &P, typename RngOf<MODEL>::T &rng, float3 seed,
                          DirState dir, float *frame, float *out, const WarpBufs &W,
                          const int *partner_sh, int lane) {
+    if constexpr (MODEL == PROB) return prob_track(P, rng, seed, dir, out, W.odf, lane);
     const int step_frac = (MODEL == PTT) ? P.step_frac : 1;
     const double ss = P.step_size / step_frac;
     float3 pt = seed;

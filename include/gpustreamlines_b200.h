@@ -54,7 +54,8 @@ typedef struct csl_params {
     int samplm_nr;                /* ODF samples: rows of sampling_matrix (BOOT) or dimt */
     int sphere_symm;              /* SPHERE_SYMM */
     int max_sline_len;            /* MAX_SLINE_LEN, 501 in the reference (_globals.py:3) */
-    int _pad0;
+    int seed_order;               /* 0: seeds scheduled in input order; 1: scheduled in spatial
+                                     (Morton) order with per-block ranges -- same results */
     double step_size;             /* STEP_SIZE, voxels */
     double max_angle;             /* MAX_ANGLE, radians */
     double tc_threshold;          /* TC_THRESHOLD */
