@@ -38,6 +38,10 @@ sys.path.insert(0, HERE)
 
 METRIC = "tracking steps/s on 1 B200, learned+BF16 form vs plain FP32 kernel, 1M seeds"
 BYTES_PER_STEP = 8 * 724 * 4 + 8 * 4 + 12  # PMF corners + stop-map taps + point write
+# DRAM bytes (read + write) per tracking step of track_kernel<PROB>, from one ncu
+# capture of this workload at 20,000 seeds (27.25 GB over 6,372,721 steps, see
+# profiles/track_kernel_prob_81x106x76x724.md); scaled to a full launch by steps.
+TRAFFIC_BYTES_PER_STEP = 4277.0
 
 
 def parse():
@@ -49,8 +53,8 @@ def parse():
     ap.add_argument("--seeds", type=int, default=1_000_000)
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--traffic-bytes-per-step", type=float, default=None,
-                    help="DRAM bytes per tracking step from an ncu capture (optional)")
+    ap.add_argument("--traffic-bytes-per-step", type=float, default=TRAFFIC_BYTES_PER_STEP,
+                    help="DRAM bytes per tracking step from an ncu capture (0 = unknown)")
     return ap.parse_args()
 
 
@@ -268,9 +272,10 @@ def main():
     value = all_steps * args.steps / (total_ms_max / 1e3)
 
     # ---- end-to-end through the C ABI with host buffers
-    L = np.empty(nsl, dtype=np.int32)
-    S = np.empty(nsl, dtype=np.int32)
-    Pt = np.empty((npts, 3), dtype=np.float32)
+    # pinned host buffers for the results, as for the seeds
+    L = torch.empty(nsl, dtype=torch.int32).pin_memory().numpy()
+    S = torch.empty(nsl, dtype=torch.int32).pin_memory().numpy()
+    Pt = torch.empty((npts, 3), dtype=torch.float32).pin_memory().numpy()
     seeds_host = seeds_pinned.numpy()
     barrier()
     torch.cuda.synchronize()
@@ -325,7 +330,8 @@ def main():
                          "frac": achieved / peak, "traffic": traffic,
                          "kernel": "track_kernel<PROB> (pass 2)",
                          "peak_source": f"{peak_kind} MEASURED_PEAKS hbm_gbs",
-                         "algorithmic_bytes_per_step": BYTES_PER_STEP},
+                         "algorithmic_bytes_per_step": BYTES_PER_STEP,
+                         "traffic_source": "ncu dram__bytes_read+write per step at 20k seeds x steps"},
             "e2e": {"value": e2e_value, "unit": "steps/s", "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h},
             "gpu_launches": 3 * args.steps,
