@@ -51,6 +51,8 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--seeds", type=int, default=1_000_000)
+    ap.add_argument("--getter", default="prob", choices=sorted(GETTERS),
+                    help="prob = the headline workload; csa/opdt/ptt print supplementary lines")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--traffic-bytes-per-step", type=float, default=TRAFFIC_BYTES_PER_STEP,
@@ -65,15 +67,45 @@ def dist_info():
     return rank, world, local
 
 
-def build_workload(rank: int, nseeds: int):
+GETTERS = {
+    # the headline workload
+    "prob": dict(model="PROB", max_angle=45.0,
+                 label="prob getter (plain FP32), 81x106x76 PMF x 724 vertices (1.9 GB)"),
+    # supplementary lines (not the headline): the other getters on the same phantom
+    "csa": dict(model="CSA", max_angle=60.0, sh_order=8,
+                label="bootstrap CSA getter (plain FP32), sh_order 8 (45 coeffs), 81x106x76x160 DWI"),
+    "opdt": dict(model="OPDT", max_angle=60.0, sh_order=6,
+                 label="bootstrap OPDT getter (plain FP32), sh_order 6 (28 coeffs), 81x106x76x160 DWI"),
+    "ptt": dict(model="PTT", max_angle=60.0,
+                label="PTT getter, 81x106x76 ODF x 724 vertices (tiled texture), step 0.5 = 20 sub-steps"),
+}
+
+
+def build_workload(rank: int, nseeds: int, getter: str = "prob"):
     from gpustreamlines_b200.phantom import make_phantom, odf_volume, seeds_from_mask
     from gpustreamlines_b200.sphere import get_sphere
 
     ph = make_phantom((81, 106, 76), seed=1234)
     sph = get_sphere("repulsion724")
-    pmf = odf_volume(ph, sph)
+    if GETTERS[getter]["model"] in ("CSA", "OPDT"):
+        data = np.ascontiguousarray(ph.dwi, dtype=np.float32)
+    else:
+        data = odf_volume(ph, sph)
     seeds = seeds_from_mask(ph.fa, nseeds, threshold=0.3, seed=1000 + rank).astype(np.float32)
-    return ph, sph, pmf, seeds
+    return ph, sph, data, seeds
+
+
+def make_getter(getter: str, ph, sph):
+    from gpustreamlines_b200 import BootDirectionGetter, ProbDirectionGetter, PttDirectionGetter
+
+    g = GETTERS[getter]
+    if g["model"] == "CSA":
+        return BootDirectionGetter.from_dipy_csa(ph.gtab, sph, sh_order_max=g["sh_order"])
+    if g["model"] == "OPDT":
+        return BootDirectionGetter.from_dipy_opdt(ph.gtab, sph, sh_order_max=g["sh_order"])
+    if g["model"] == "PTT":
+        return PttDirectionGetter()
+    return ProbDirectionGetter()
 
 
 def measured_peaks():
@@ -137,20 +169,28 @@ class ClockSampler:
                 "samples": len(self.rows)}
 
 
-def cpu_baseline(ph, sph, pmf, seeds, seconds: float, threads: int | None = None):
+def cpu_baseline(ph, sph, data, seeds, seconds: float, threads: int | None = None,
+                 getter: str = "prob", dg=None):
     """The oracle (CPU restatement of the reference) on a bounded seed sample."""
     import math as _m
 
     from oracle import api
 
+    g = GETTERS[getter]
+    if g["model"] == "PTT":
+        raise RuntimeError("the oracle restates the prob and bootstrap getters only")
     threads = threads or os.cpu_count() or 1
-    inp = dict(case=dict(model="PROB", step=0.5, max_angle=45.0, fa_thr=0.1, rel=0.25, min_sep=45.0,
-                         rng_seed=0),
-               dataf=pmf, stop_map=np.ascontiguousarray(ph.fa, dtype=np.float32),
+    inp = dict(case=dict(model=g["model"], step=0.5, max_angle=g["max_angle"], fa_thr=0.1, rel=0.25,
+                         min_sep=45.0, rng_seed=0),
+               dataf=data, stop_map=np.ascontiguousarray(ph.fa, dtype=np.float32),
                vertices=np.ascontiguousarray(sph.vertices, dtype=np.float32),
                edges=np.ascontiguousarray(sph.edges, dtype=np.int32))
-    o = api.Oracle(inp, cos_max_angle=np.float32(_m.cos(np.float32(_m.radians(45.0)))))
-    n = 256
+    if g["model"] in ("CSA", "OPDT"):
+        for k in ("H", "R", "delta_b", "delta_q", "sampling_matrix", "b0s_mask", "min_signal"):
+            inp[k] = getattr(dg, k)
+    ang = np.float32(_m.radians(g["max_angle"]))
+    o = api.Oracle(inp, cos_max_angle=np.float32(_m.cos(ang)))
+    n = 256 if g["model"] == "PROB" else 64
     steps = 0
     elapsed = 0.0
     used = 0
@@ -165,7 +205,7 @@ def cpu_baseline(ph, sph, pmf, seeds, seconds: float, threads: int | None = None
         if elapsed >= seconds or used >= len(seeds):
             break
         rate = used / max(elapsed, 1e-9)
-        n = int(min(max(256, rate * (seconds - elapsed)), len(seeds) - used))
+        n = int(min(max(64, rate * (seconds - elapsed)), len(seeds) - used))
     return dict(value=steps / elapsed, unit="steps/s", cores=threads, kind="port",
                 sample=f"{used} of the benchmark's seeds ({steps} steps, {elapsed:.1f} s)")
 
@@ -173,13 +213,14 @@ def cpu_baseline(ph, sph, pmf, seeds, seconds: float, threads: int | None = None
 def run_reference(args, rank, world):
     if rank != 0:
         return 0
-    ph, sph, pmf, seeds = build_workload(0, args.seeds)
+    ph, sph, data, seeds = build_workload(0, args.seeds, args.getter)
+    dg = make_getter(args.getter, ph, sph)
     threads = os.cpu_count() or 1
     per = args.cpu_seconds / max(args.steps + args.warmup, 1)
     vals = []
     for i in range(args.warmup + args.steps):
         sub = seeds[(i * 997) % max(len(seeds) - 50_000, 1):]
-        r = cpu_baseline(ph, sph, pmf, sub, max(per, 2.0), threads)
+        r = cpu_baseline(ph, sph, data, sub, max(per, 2.0), threads, args.getter, dg)
         if i >= args.warmup:
             vals.append(r)
     v = float(np.mean([r["value"] for r in vals]))
@@ -187,8 +228,8 @@ def run_reference(args, rank, world):
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": None,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic phantom (Stanford HARDI shapes)",
-            "config": {"workload": "prob getter, 81x106x76x724 PMF, 1M seeds (bounded CPU sample)",
-                       "seeds": args.seeds},
+            "config": {"workload": f"{GETTERS[args.getter]['label']}, {args.seeds} seeds "
+                                   "(bounded CPU sample per step)", "seeds": args.seeds},
             "cpu_baseline": {"value": v, "unit": "steps/s", "cores": threads, "kind": "port",
                              "sample": "; ".join(r["sample"] for r in vals)},
             "e2e": {"value": v, "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
@@ -214,11 +255,14 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
                                 device_id=torch.device("cuda", local))
 
-    from gpustreamlines_b200 import ProbDirectionGetter, Tracker
+    from gpustreamlines_b200 import Tracker
 
-    ph, sph, pmf, seeds = build_workload(rank, args.seeds)
-    tracker = Tracker(ProbDirectionGetter(), pmf, ph.fa, 0.1, sph.vertices, sph.edges,
-                      max_angle=math.radians(45), step_size=0.5, ngpus=1, device_offset=local)
+    gcfg = GETTERS[args.getter]
+    ph, sph, data, seeds = build_workload(rank, args.seeds, args.getter)
+    dg = make_getter(args.getter, ph, sph)
+    tracker = Tracker(dg, data, ph.fa, 0.1, sph.vertices, sph.edges,
+                      max_angle=math.radians(gcfg["max_angle"]), step_size=0.5, ngpus=1,
+                      device_offset=local)
     tracker.__enter__()
     h = tracker.handles[0]
     stream = torch.cuda.Stream(device=local)
@@ -298,15 +342,42 @@ def main():
 
     peak, peak_kind = measured_peaks()
     p2 = float(np.mean(pass2_ms))
-    achieved = steps_per_batch * BYTES_PER_STEP / (p2 / 1e3) / 1e9
+    model = gcfg["model"]
+    if model == "PTT":
+        # dependent texture fetches: reported as sub-steps/s, no byte roofline
+        bytes_per_step = None
+        achieved = None
+    elif model in ("CSA", "OPDT"):
+        bytes_per_step = 8 * data.shape[3] * 4 + 8 * 4 + 12  # DWI corners + stop taps + point
+        achieved = steps_per_batch * bytes_per_step / (p2 / 1e3) / 1e9
+    else:
+        bytes_per_step = BYTES_PER_STEP
+        achieved = steps_per_batch * BYTES_PER_STEP / (p2 / 1e3) / 1e9
     traffic = None
-    if args.traffic_bytes_per_step:
+    if args.traffic_bytes_per_step and model == "PROB":
         traffic = args.traffic_bytes_per_step * steps_per_batch
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": None if achieved is None else achieved / peak, "traffic": traffic,
+                "kernel": f"track_kernel<{model}> (pass 2)",
+                "peak_source": f"{peak_kind} MEASURED_PEAKS hbm_gbs",
+                "algorithmic_bytes_per_step": bytes_per_step}
+    if model == "PROB":
+        roofline["traffic_source"] = "ncu dram__bytes_read+write per step at 20k seeds x steps"
+    extra = {}
+    if model == "PTT":
+        frac = int(np.round(0.5 / dg.target_short_step))  # propagation sub-steps per point
+        extra["sub_steps_per_s"] = value * frac
+        extra["step_frac"] = frac
+    if model in ("CSA", "OPDT"):
+        nc = dg.delta_nr
+        hr = int((dg.b0s_mask == 0).sum())
+        k = 2 if model == "OPDT" else 1
+        extra["flop_per_attempt"] = 2 * 2 * hr * hr + 2 * nc * hr * k + 2 * nc * dg.sampling_matrix.shape[0]
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
-            cpu = cpu_baseline(ph, sph, pmf, seeds, args.cpu_seconds)
+            cpu = cpu_baseline(ph, sph, data, seeds, args.cpu_seconds, getter=args.getter, dg=dg)
         except Exception as e:  # the oracle is optional on the GPU box
             cpu = {"value": None, "unit": "steps/s", "cores": 0, "kind": "port",
                    "sample": f"unavailable: {e}"}
@@ -317,21 +388,16 @@ def main():
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic phantom with Stanford HARDI shapes (seeded), random seeds in FA>0.3",
-            "config": {"workload": "prob getter (plain FP32), 81x106x76 PMF x 724 vertices (1.9 GB), "
-                                   f"{args.seeds} seeds per GPU, step 0.5, max angle 45",
+            "config": {"workload": f"{gcfg['label']}, {args.seeds} seeds per GPU, step 0.5, "
+                                   f"max angle {gcfg['max_angle']:g}",
                        "global_batch": args.seeds * world, "seeds_per_gpu": args.seeds,
                        "streamlines_per_gpu": nsl, "steps_per_gpu": int(steps_per_batch),
                        "parallelism": f"seed shards x{world}",
-                       "l2": "inputs (1.9 GB PMF) larger than L2; no flush",
+                       "l2": f"inputs ({data.nbytes / 1e9:.2f} GB volume) larger than L2; no flush",
                        "pass1_ms": float(np.mean(pass1_ms)), "pass2_ms": p2,
                        "compact_ms": float(np.mean(compact_ms)),
-                       "streamlines_per_s": nsl * world * args.steps / (total_ms_max / 1e3)},
-            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "traffic": traffic,
-                         "kernel": "track_kernel<PROB> (pass 2)",
-                         "peak_source": f"{peak_kind} MEASURED_PEAKS hbm_gbs",
-                         "algorithmic_bytes_per_step": BYTES_PER_STEP,
-                         "traffic_source": "ncu dram__bytes_read+write per step at 20k seeds x steps"},
+                       "streamlines_per_s": nsl * world * args.steps / (total_ms_max / 1e3), **extra},
+            "roofline": roofline,
             "e2e": {"value": e2e_value, "unit": "steps/s", "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h},
             "gpu_launches": 3 * args.steps,

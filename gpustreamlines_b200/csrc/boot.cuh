@@ -29,12 +29,15 @@ struct BootSmem {
 
 constexpr float kN0Const = 0.28209479177387814f;  // .5 / sqrt(pi)
 
-// dst[i] = sum_j v[j] * M[i*m + j]   (ndotp_d, boot.cu:195-230); only lane 0 writes
-template <int KIND>  // 0 plain, 1 OPDT transform, 2 CSA transform
-__device__ __forceinline__ void ndotp_rows(int nrows, int m, const float *v_sh,
-                                           const float *__restrict__ M, float *dst, int lane) {
+// dst[i] = sum_j v[j] * M[i*m + j]   (ndotp_d, boot.cu:195-230).
+// NPER = compile-time bound on the elements per lane (m <= 32 * NPER), so the
+// unrolled loops carry no dead iterations; the arithmetic of each row does
+// not depend on NPER.
+template <int KIND, int NPER>  // KIND: 0 plain, 1 OPDT transform, 2 CSA transform
+__device__ __forceinline__ void ndotp_rows_n(int nrows, int m, const float *v_sh,
+                                             const float *__restrict__ M, float *dst, int lane) {
     // transformed source values of this lane (the transform is per element)
-    constexpr int kMaxPer = 16;  // m <= 512
+    constexpr int kMaxPer = NPER;
     float sv[kMaxPer];
     const int nper = (m + kWarp - 1) / kWarp;
 #pragma unroll
@@ -56,46 +59,50 @@ __device__ __forceinline__ void ndotp_rows(int nrows, int m, const float *v_sh,
             }
         }
     }
-    int i = 0;
-    for (; i + 4 <= nrows; i += 4) {
-        float t0 = 0.0f, t1 = 0.0f, t2 = 0.0f, t3 = 0.0f;
-        const float *r0 = M + (size_t)i * m;
+    // 32 rows at a time: lane l accumulates its lane-strided partial of every
+    // row, then a transposing xor butterfly (16, 8, 4, 2, 1) leaves the sum of
+    // row r0 + l in lane l.  At each level a lane adds its own partial to its
+    // partner's for the half of the rows it keeps: the same pairs, in the same
+    // association, as the reference's shfl_down tree, which only lane 0 reads.
+    const int npr = nper;
+    for (int r0 = 0; r0 < nrows; r0 += kWarp) {
+        float v[kWarp];
 #pragma unroll
-        for (int q = 0; q < kMaxPer; q++) {
-            const int j = q * kWarp + lane;
-            if (q < nper && j < m) {
-                t0 += sv[q] * __ldg(r0 + j);
-                t1 += sv[q] * __ldg(r0 + m + j);
-                t2 += sv[q] * __ldg(r0 + 2 * m + j);
-                t3 += sv[q] * __ldg(r0 + 3 * m + j);
+        for (int r = 0; r < kWarp; r++) {
+            float t = 0.0f;
+            if (r0 + r < nrows) {
+                const float *row = M + (size_t)(r0 + r) * m;
+#pragma unroll
+                for (int q = 0; q < kMaxPer; q++) {
+                    const int j = q * kWarp + lane;
+                    if (q < npr && j < m) t += sv[q] * __ldg(row + j);
+                }
+            }
+            v[r] = t;
+        }
+#pragma unroll
+        for (int o = kWarp / 2; o; o >>= 1) {
+            const bool up = (lane & o) != 0;
+#pragma unroll
+            for (int i = 0; i < o; i++) {
+                const float send = up ? v[i] : v[i + o];
+                const float keep = up ? v[i + o] : v[i];
+                v[i] = keep + __shfl_xor_sync(FULL, send, o);
             }
         }
-#pragma unroll
-        for (int o = 16; o; o >>= 1) {
-            t0 += __shfl_down_sync(FULL, t0, o);
-            t1 += __shfl_down_sync(FULL, t1, o);
-            t2 += __shfl_down_sync(FULL, t2, o);
-            t3 += __shfl_down_sync(FULL, t3, o);
-        }
-        if (lane == 0) {
-            dst[i] = t0;
-            dst[i + 1] = t1;
-            dst[i + 2] = t2;
-            dst[i + 3] = t3;
-        }
+        if (r0 + lane < nrows) dst[r0 + lane] = v[0];
     }
-    for (; i < nrows; i++) {
-        float t0 = 0.0f;
-        const float *r0 = M + (size_t)i * m;
-#pragma unroll
-        for (int q = 0; q < kMaxPer; q++) {
-            const int j = q * kWarp + lane;
-            if (q < nper && j < m) t0 += sv[q] * __ldg(r0 + j);
-        }
-#pragma unroll
-        for (int o = 16; o; o >>= 1) t0 += __shfl_down_sync(FULL, t0, o);
-        if (lane == 0) dst[i] = t0;
-    }
+}
+
+template <int KIND>
+__device__ __forceinline__ void ndotp_rows(int nrows, int m, const float *v_sh,
+                                           const float *__restrict__ M, float *dst, int lane) {
+    if (m <= 2 * kWarp)
+        ndotp_rows_n<KIND, 2>(nrows, m, v_sh, M, dst, lane);
+    else if (m <= 5 * kWarp)
+        ndotp_rows_n<KIND, 5>(nrows, m, v_sh, M, dst, lane);
+    else
+        ndotp_rows_n<KIND, 16>(nrows, m, v_sh, M, dst, lane);
 }
 
 // maskGet (boot.cu:52-83): compact entries with mask == 0

@@ -24,6 +24,9 @@
 #include "track.cuh"
 
 // resident 256-thread blocks per SM the probabilistic tracker is compiled for
+#ifndef CSL_BOOT_MIN_BLOCKS
+#define CSL_BOOT_MIN_BLOCKS 2
+#endif
 #ifndef CSL_PROB_MIN_BLOCKS
 #define CSL_PROB_MIN_BLOCKS 4
 #endif
@@ -111,7 +114,8 @@ __global__ void block_ranges_kernel(int n, int nblocks, int *next, int *end) {
 }
 
 template <int MODEL>
-__global__ void __launch_bounds__(256, MODEL == PROB ? CSL_PROB_MIN_BLOCKS : 1) track_kernel(DevParams P, BatchArgs B, const int *partner,
+__global__ void __launch_bounds__(256, MODEL == PROB ? CSL_PROB_MIN_BLOCKS
+                                         : (MODEL == PTT ? 1 : CSL_BOOT_MIN_BLOCKS)) track_kernel(DevParams P, BatchArgs B, const int *partner,
                                                     const int *__restrict__ npeaks,
                                                     const short *__restrict__ peaks, int max_store,
                                                     const int *__restrict__ sl_off, int *out_len,
