@@ -74,6 +74,9 @@ GETTERS = {
     # supplementary lines (not the headline): the other getters on the same phantom
     "csa": dict(model="CSA", max_angle=60.0, sh_order=8,
                 label="bootstrap CSA getter (plain FP32), sh_order 8 (45 coeffs), 81x106x76x160 DWI"),
+    "csa_bf16x3": dict(model="CSA", max_angle=60.0, sh_order=8, fit="bf16x3",
+                       label="bootstrap CSA getter, batched tensor-core fit (BF16x3, FP32 accumulate), "
+                             "sh_order 8 (45 coeffs), 81x106x76x160 DWI"),
     "opdt": dict(model="OPDT", max_angle=60.0, sh_order=6,
                  label="bootstrap OPDT getter (plain FP32), sh_order 6 (28 coeffs), 81x106x76x160 DWI"),
     "ptt": dict(model="PTT", max_angle=60.0,
@@ -100,7 +103,8 @@ def make_getter(getter: str, ph, sph):
 
     g = GETTERS[getter]
     if g["model"] == "CSA":
-        return BootDirectionGetter.from_dipy_csa(ph.gtab, sph, sh_order_max=g["sh_order"])
+        return BootDirectionGetter.from_dipy_csa(ph.gtab, sph, sh_order_max=g["sh_order"],
+                                                 fit=g.get("fit", "fp32"))
     if g["model"] == "OPDT":
         return BootDirectionGetter.from_dipy_opdt(ph.gtab, sph, sh_order_max=g["sh_order"])
     if g["model"] == "PTT":
@@ -363,6 +367,8 @@ def main():
                 "algorithmic_bytes_per_step": bytes_per_step}
     if model == "PROB":
         roofline["traffic_source"] = "ncu dram__bytes_read+write per step at 20k seeds x steps"
+    if gcfg.get("fit") == "bf16x3":
+        roofline["kernel"] = "boot_batch_kernel (pass 2, tcgen05 BF16x3)"
     extra = {}
     if model == "PTT":
         frac = int(np.round(0.5 / dg.target_short_step))  # propagation sub-steps per point

@@ -35,7 +35,7 @@ class CslParams(C.Structure):
         ("step_size", C.c_double), ("max_angle", C.c_double), ("tc_threshold", C.c_double),
         ("relative_peak_thresh", C.c_double), ("min_separation_angle", C.c_double),
         ("pmf_threshold", C.c_double), ("rng_seed", C.c_ulonglong),
-        ("min_signal", C.c_double), ("delta_nr", C.c_int), ("_pad1", C.c_int),
+        ("min_signal", C.c_double), ("delta_nr", C.c_int), ("boot_fit", C.c_int),
         ("odf_lut_res", C.c_int), ("step_frac", C.c_int),
         ("probe_step_size", C.c_double), ("probe_quality", C.c_double),
         ("max_curvature", C.c_double),

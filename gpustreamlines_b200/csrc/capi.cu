@@ -77,6 +77,13 @@ struct csl_tracker {
     DevBuf<unsigned char> scan_tmp, sort_tmp;
     DevBuf<uint32_t> mkeys, mkeys_sorted;
     DevBuf<int> mvals, perm, blk_next, blk_end;
+    // batched bootstrap fit (boot_fit == 1)
+    BootBatchGeom bgeom{};
+    DevBuf<unsigned char> bb_B1, bb_B2, bb_B3;
+    DevBuf<int> bb_nbpos, bb_sl_seed, bb_half_len, bb_hq;
+    DevBuf<short> bb_sl_vert;
+    DevBuf<long long> bb_half_off;
+    DevBuf<float> bb_odf, bb_pts;
     long long *host_stage = nullptr;  // pinned 16-byte staging for the two totals
     long long last_n = -1, nsl = 0, npts = 0;
     int ok_batch = 0;
@@ -221,6 +228,19 @@ static void release_all(csl_tracker *t) {
     t->pt_off.release();
     t->pool_count.release();
     t->scan_tmp.release();
+    t->sort_tmp.release();
+    t->mkeys.release();
+    t->mkeys_sorted.release();
+    DevBuf<int> *ib2[] = {&t->mvals, &t->perm, &t->blk_next, &t->blk_end, &t->bb_nbpos,
+                          &t->bb_sl_seed, &t->bb_half_len, &t->bb_hq};
+    for (auto *b : ib2) b->release();
+    t->bb_B1.release();
+    t->bb_B2.release();
+    t->bb_B3.release();
+    t->bb_sl_vert.release();
+    t->bb_half_off.release();
+    t->bb_odf.release();
+    t->bb_pts.release();
     for (auto &e : t->ev)
         if (e) cudaEventDestroy(e);
     if (t->host_stage) cudaFreeHost(t->host_stage);
@@ -252,6 +272,13 @@ static int validate(const csl_params *p, const csl_inputs *in, csl_tracker *t) {
         if (p->samplm_nr != p->nvertices)
             return fail(t, CSL_E_INVALID, "sampling_matrix rows (%d) must equal sphere vertices (%d)",
                         p->samplm_nr, p->nvertices);
+        if (p->boot_fit != 0 && p->boot_fit != 1) return fail(t, CSL_E_INVALID, "boot_fit must be 0 or 1");
+        if (p->boot_fit == 1) {
+            if (p->model != CSL_MODEL_CSA)
+                return fail(t, CSL_E_INVALID, "the batched tensor-core fit (boot_fit=1) supports the CSA model");
+            if (p->delta_nr > 64) return fail(t, CSL_E_INVALID, "boot_fit=1 supports at most 64 SH coefficients");
+            if (p->samplm_nr > 768) return fail(t, CSL_E_INVALID, "boot_fit=1 supports at most 768 sphere samples");
+        }
     } else {
         if (p->nvertices != p->dimt)
             return fail(t, CSL_E_INVALID,
@@ -377,6 +404,25 @@ int csl_create(const csl_params *params, const csl_inputs *inputs, int device, c
             P.delta_q = t->delta_q.p;
             P.sampling = t->sampling.p;
             P.b0s_mask = t->b0s.p;
+            if (p.boot_fit == 1) {
+                if (hr > 160)
+                    return fail(t, CSL_E_INVALID, "boot_fit=1 supports at most 160 non-b0 volumes, got %d", hr);
+                std::vector<int> nbpos(p.dimt);
+                int k = 0;
+                for (int i = 0; i < p.dimt; i++) nbpos[i] = inputs->b0s_mask[i] ? -1 : k++;
+                const BootBatchGeom g = boot_batch_geom(P, hr, p.dimt - hr);
+                t->bgeom = g;
+                if ((r = upload(t, t->bb_nbpos, nbpos.data(), nbpos.size()))) return r;
+                CK(t->bb_B1.ensure((size_t)g.nchunk1 * g.b1_chunk));
+                CK(t->bb_B2.ensure((size_t)g.b2_bytes));
+                CK(t->bb_B3.ensure((size_t)g.nchunk3 * g.b3_chunk));
+                CK(t->bb_hq.ensure(1));
+                CK(launch_boot_batch_pack(P, g, t->bb_B1.p, t->bb_B2.p, t->bb_B3.p, t->own_stream));
+                CK(boot_batch_set_smem(g));
+                const size_t slots = (size_t)t->nsm * 128;
+                CK(t->bb_odf.ensure(slots * g.vstride));
+                CK(t->bb_pts.ensure(slots * (size_t)p.max_sline_len * 3));
+            }
         }
         if (p.model == PROB) {
             CK(t->cone.ensure((size_t)2 * P.nvert * P.nch));
@@ -441,6 +487,96 @@ int csl_destroy(csl_tracker *t) {
     return CSL_OK;
 }
 
+// Pass 2 with the batched tensor-core fit (boot_fit == 1): streamline halves
+// are tracked independently, 128 per CTA, and joined afterwards.  Returns
+// kUsePerWarpPath when a seed has more initial directions than pass 1 stores
+// (the per-warp path recomputes them).
+static constexpr int kUsePerWarpPath = 1;
+
+static int run_boot_batch(csl_tracker *t, const float *seeds_dev, int ni, int nsl, long long rng_base,
+                          cudaStream_t st) {
+    const DevParams &P = t->P;
+    const BootBatchGeom &g = t->bgeom;
+    CK(t->bb_sl_seed.ensure((size_t)nsl + 1));
+    CK(t->bb_sl_vert.ensure((size_t)nsl + 1));
+    CK(t->bb_half_len.ensure((size_t)2 * nsl + 2));
+    CK(t->bb_half_off.ensure((size_t)2 * nsl + 2));
+    CK(cudaMemsetAsync(t->status.p, 0, sizeof(int), st));
+    CK(launch_boot_batch_prep(t->npeaks.p, t->sl_off.p, t->peaks.p, kMaxStoredPeaksPerSeed, ni,
+                              t->bb_sl_seed.p, t->bb_sl_vert.p, t->status.p, st));
+    CK(cudaMemcpyAsync(t->host_stage, t->status.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    if ((int)(t->host_stage[0] & 0xffffffff) & ST_PEAKS_OVERFLOW) return kUsePerWarpPath;
+
+    unsigned long long want = std::max<unsigned long long>(t->pool.cap / 3, (unsigned long long)nsl * 96ull);
+    for (int attempt = 0; attempt < 2; attempt++) {
+        CK(t->pool.ensure(want * 3));
+        BootBatchArgs A{};
+        A.B1g = t->bb_B1.p;
+        A.B2g = t->bb_B2.p;
+        A.B3g = t->bb_B3.p;
+        A.nbpos = t->bb_nbpos.p;
+        A.seeds = seeds_dev;
+        A.sl_seed = t->bb_sl_seed.p;
+        A.sl_vert = t->bb_sl_vert.p;
+        A.nsl = nsl;
+        A.rng_base = rng_base;
+        A.hq = t->bb_hq.p;
+        A.odf = t->bb_odf.p;
+        A.pts = t->bb_pts.p;
+        A.pool_count = t->pool_count.p;
+        A.pool = t->pool.p;
+        A.pool_cap = t->pool.cap / 3;
+        A.half_len = t->bb_half_len.p;
+        A.half_off = t->bb_half_off.p;
+        A.status = t->status.p;
+        CK(cudaMemsetAsync(t->bb_hq.p, 0, sizeof(int), st));
+        CK(cudaMemsetAsync(t->status.p, 0, sizeof(int), st));
+        CK(cudaMemsetAsync(t->pool_count.p, 0, sizeof(unsigned long long), st));
+        CK(cudaEventRecord(t->ev[2], st));
+        if (nsl > 0) CK(launch_boot_batch(P, g, A, t->partner.p, t->nsm, st));
+        CK(cudaEventRecord(t->ev[3], st));
+        t->pass2_runs++;
+        CK(cudaMemcpyAsync(t->host_stage, t->status.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+        CK(cudaMemcpyAsync(t->host_stage + 1, t->pool_count.p, sizeof(unsigned long long),
+                           cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        const int status = (int)(t->host_stage[0] & 0xffffffff);
+        const unsigned long long used = (unsigned long long)t->host_stage[1];
+        if (status & ST_WAIT_TIMEOUT) return fail(t, CSL_E_KERNEL, "tensor-core pipeline wait timed out");
+        if (!(status & ST_POOL_OVERFLOW)) break;
+        if (attempt == 1) return fail(t, CSL_E_KERNEL, "point pool overflow after resize");
+        want = used + used / 8 + 1024;
+    }
+
+    // join the halves, scan the lengths, gather
+    CK(launch_boot_batch_join(t->bb_half_len.p, t->bb_sl_seed.p, nsl, t->out_len.p, t->out_seed.p, st));
+    CK(cudaMemsetAsync(t->out_len.p + nsl, 0, sizeof(int), st));
+    size_t tmpb = 0;
+    CK(scan_temp_bytes(nsl + 1, &tmpb));
+    if (tmpb > t->scan_tmp.cap) {
+        CK(cudaStreamSynchronize(st));
+        CK(t->scan_tmp.ensure(tmpb));
+    }
+    CK(exclusive_scan_i64(t->scan_tmp.p, t->scan_tmp.cap, t->out_len.p, t->pt_off.p, nsl + 1, st));
+    CK(cudaMemcpyAsync(t->host_stage, t->pt_off.p + nsl, sizeof(long long), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    const long long npts = t->host_stage[0];
+    t->npts = npts;
+    CK(t->points.ensure((size_t)npts * 3 + 3));
+    if (nsl > 0)
+        CK(launch_gather_halves(t->pool.p, t->bb_half_off.p, t->bb_half_len.p, t->pt_off.p, nsl,
+                                t->points.p, t->nsm * 8, st));
+    CK(cudaEventRecord(t->ev[4], st));
+    CK(cudaStreamSynchronize(st));
+    CK(cudaEventElapsedTime(&t->ms[0], t->ev[0], t->ev[1]));
+    CK(cudaEventElapsedTime(&t->ms[1], t->ev[1], t->ev[2]));
+    CK(cudaEventElapsedTime(&t->ms[2], t->ev[2], t->ev[3]));
+    CK(cudaEventElapsedTime(&t->ms[3], t->ev[3], t->ev[4]));
+    t->ok_batch = 1;
+    return CSL_OK;
+}
+
 static int run_batch(csl_tracker *t, const float *seeds_dev, long long n, long long rng_base,
                      cudaStream_t st) {
     const DevParams &P = t->P;
@@ -481,6 +617,11 @@ static int run_batch(csl_tracker *t, const float *seeds_dev, long long n, long l
     CK(t->out_seed.ensure((size_t)nsl + 1));
     CK(t->out_src.ensure((size_t)nsl + 1));
     CK(t->pt_off.ensure((size_t)nsl + 1));
+
+    if (t->hp.boot_fit == 1 && P.model == CSA) {
+        const int r = run_boot_batch(t, seeds_dev, ni, nsl, rng_base, st);
+        if (r != kUsePerWarpPath) return r;
+    }
 
     // pass 2 (re-run once with an exact pool size if the guess was short)
     const long long warps_needed = n;

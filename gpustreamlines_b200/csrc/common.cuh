@@ -78,7 +78,11 @@ struct BatchArgs {
     int *status;                        // error/overflow flags
 };
 
-enum StatusBits { ST_POOL_OVERFLOW = 1 };
+enum StatusBits {
+    ST_POOL_OVERFLOW = 1,   // point pool too small: the batch is re-run with an exact size
+    ST_PEAKS_OVERFLOW = 2,  // a seed has more initial directions than pass 1 stores
+    ST_WAIT_TIMEOUT = 4,    // a bounded wait on an mbarrier gave up (never expected)
+};
 
 // ---------------------------------------------------------------------------
 // warp reductions (utils.cu:1-80): lane-strided partial, then xor butterfly

@@ -37,6 +37,50 @@ cudaError_t launch_device_cos(float a, float b, float *out, cudaStream_t st);
 cudaError_t launch_philox_stream(unsigned long long seed, unsigned long long subseq,
                                  unsigned long long offset, long long n, unsigned *out,
                                  cudaStream_t st);
+// ---- batched bootstrap fit on the tensor cores (boot_batch.cu)
+struct BootBatchGeom {
+    int hr, nb0;        // non-b0 / b0 volumes
+    int HP, N1;         // hr padded to 32; rows of [R ; H] = 2 HP
+    int C, N2;          // SH coefficients, padded to 16
+    int V, nchunk1, nchunk3, vstride;
+    int b1_chunk, b2_bytes, b3_chunk;  // bytes of one packed operand chunk (hi + lo)
+    int r0, r1, r2, smem;              // shared-memory regions and total
+};
+
+struct BootBatchArgs {
+    const unsigned char *B1g;  // [HP/32][2][2HP x 32] packed [R ; H]
+    const unsigned char *B2g;  // [2][N2 x HP] packed delta_q
+    const unsigned char *B3g;  // [nchunk3][2][256 x N2] packed sampling matrix
+    const int *nbpos;          // [T] index among the non-b0 volumes, -1 for a b0
+    const float *seeds;
+    const int *sl_seed;        // streamline -> seed (batch-local)
+    const short *sl_vert;      // streamline -> initial vertex
+    int nsl;
+    long long rng_base;
+    int *hq;                   // atomic queue of streamline halves
+    float *odf;                // [grid * 128][vstride] ODF rows
+    float *pts;                // [grid * 128][max_sline_len * 3] points of the running halves
+    unsigned long long *pool_count;
+    float *pool;
+    unsigned long long pool_cap;
+    int *half_len;             // [2 nsl] points per half (seed included)
+    long long *half_off;       // [2 nsl] pool offset of each half (-1 when the pool overflowed)
+    int *status;
+};
+
+BootBatchGeom boot_batch_geom(const DevParams &P, int hr, int nb0);
+cudaError_t launch_boot_batch_pack(const DevParams &P, const BootBatchGeom &g, void *B1g, void *B2g,
+                                   void *B3g, cudaStream_t st);
+cudaError_t launch_boot_batch_prep(const int *npeaks, const int *sl_off, const short *peaks, int max_store,
+                                   int n, int *sl_seed, short *sl_vert, int *status, cudaStream_t st);
+cudaError_t launch_boot_batch_join(const int *half_len, const int *sl_seed, int nsl, int *out_len,
+                                   int *out_seed, cudaStream_t st);
+cudaError_t launch_gather_halves(const float *pool, const long long *half_off, const int *half_len,
+                                 const long long *pt_off, int nsl, float *out, int grid, cudaStream_t st);
+cudaError_t boot_batch_set_smem(const BootBatchGeom &g);
+cudaError_t launch_boot_batch(const DevParams &P, const BootBatchGeom &g, const BootBatchArgs &A,
+                              const int *partner, int grid, cudaStream_t st);
+
 cudaError_t scan_temp_bytes(int n, size_t *bytes);
 // Morton-sort the seeds (perm = position -> seed) and split the order into
 // per-block ranges; with tmp == nullptr only reports the sort's temp size.

@@ -11,9 +11,8 @@
 // descriptor this is leading-byte offset (next k group) = rows * 16 and
 // stride-byte offset (next 8 rows) = 128.
 //
-// Every wait is bounded: mbar_wait gives up after a fixed number of polls and
-// reports it, so a lost arrival ends the kernel with an error status instead
-// of a hang.
+// Every wait is bounded: mbar_wait gives up after two seconds and reports it,
+// so a lost arrival ends the kernel with an error status instead of a hang.
 #pragma once
 #include <cstdint>
 
@@ -49,15 +48,24 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
     return ok != 0;
 }
 
-// Bounded wait for the phase with the given parity to complete.  Returns
-// false after kMbarPolls polls; each poll may itself suspend the thread for a
-// hardware-defined time slice, so the bound is well above any legitimate wait.
-constexpr long long kMbarPolls = 1ll << 24;
+__device__ __forceinline__ uint64_t globaltimer_ns() {
+    uint64_t t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// Bounded wait for the phase with the given parity to complete: gives up and
+// returns false after kMbarWaitNs nanoseconds of wall time, far above any
+// legitimate wait (a copy of a few KB or a batch of MMAs takes microseconds).
+constexpr uint64_t kMbarWaitNs = 2000000000ull;
 
 __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity) {
-    for (long long i = 0; i < kMbarPolls; i++)
+    if (mbar_try_wait(bar, parity)) return true;
+    const uint64_t t0 = globaltimer_ns();
+    for (;;) {
         if (mbar_try_wait(bar, parity)) return true;
-    return false;
+        if (globaltimer_ns() - t0 > kMbarWaitNs) return false;
+    }
 }
 
 // ---- bulk copy (global -> this CTA's shared memory, completes on an mbarrier)

@@ -57,7 +57,16 @@ class BootDirectionGetter(GPUDirectionGetter):
 
     def __init__(self, model_type: str, min_signal: float, H: np.ndarray, R: np.ndarray,
                  delta_b: np.ndarray, delta_q: np.ndarray, sampling_matrix: np.ndarray,
-                 b0s_mask: np.ndarray):
+                 b0s_mask: np.ndarray, *, fit: str = "fp32"):
+        """``fit`` (keyword only, not in the reference): "fp32" runs the
+        reference's per-warp FP32 fit with identical results; "bf16x3" runs the
+        batched tensor-core fit (CSA model), 128 streamline halves per CTA with
+        BF16x3 products and FP32 accumulation."""
+        if fit not in ("fp32", "bf16x3"):
+            raise ValueError(f"Invalid fit {fit!r}, must be one of 'fp32', 'bf16x3'")
+        if fit == "bf16x3" and model_type.upper() != "CSA":
+            raise ValueError("the batched tensor-core fit (fit='bf16x3') supports the CSA model")
+        self.fit = fit
         if model_type.upper() == "OPDT":
             self.model_type = _lib.MODEL_OPDT
         elif model_type.upper() == "CSA":
@@ -76,13 +85,15 @@ class BootDirectionGetter(GPUDirectionGetter):
 
     @classmethod
     def from_dipy_opdt(cls, gtab, sphere, sh_order_max=6, full_basis=False, sh_lambda=0.006,
-                       min_signal=1):
-        return cls(**_shm.prepare_opdt(gtab, sphere, sh_order_max, full_basis, sh_lambda, min_signal))
+                       min_signal=1, *, fit="fp32"):
+        return cls(**_shm.prepare_opdt(gtab, sphere, sh_order_max, full_basis, sh_lambda, min_signal),
+                   fit=fit)
 
     @classmethod
     def from_dipy_csa(cls, gtab, sphere, sh_order_max=6, full_basis=False, sh_lambda=0.006,
-                      min_signal=1):
-        return cls(**_shm.prepare_csa(gtab, sphere, sh_order_max, full_basis, sh_lambda, min_signal))
+                      min_signal=1, *, fit="fp32"):
+        return cls(**_shm.prepare_csa(gtab, sphere, sh_order_max, full_basis, sh_lambda, min_signal),
+                   fit=fit)
 
     def fill(self, params, inputs, tracker, keep):
         hr = int((self.b0s_mask == 0).sum())
@@ -95,6 +106,7 @@ class BootDirectionGetter(GPUDirectionGetter):
         if len(self.b0s_mask) != tracker.dimt:
             raise ValueError("b0s_mask length must match the last dimension of dataf")
         params.model = self.model_type
+        params.boot_fit = 1 if self.fit == "bf16x3" else 0
         params.min_signal = float(self.min_signal)
         params.delta_nr = self.delta_nr
         params.samplm_nr = int(self.sampling_matrix.shape[0])

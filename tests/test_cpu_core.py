@@ -149,3 +149,18 @@ def test_phantom_is_deterministic():
     s1 = seeds_from_mask(a.fa, 50, seed=2)
     s2 = seeds_from_mask(a.fa, 50, seed=2)
     assert np.array_equal(s1, s2)
+
+
+def test_boot_fit_option_validation():
+    """fit='bf16x3' is the batched tensor-core CSA fit; other models and names are rejected."""
+    from gpustreamlines_b200 import BootDirectionGetter
+    from oracle import cases
+
+    inp = cases.inputs("csa_s")
+    args = (inp["H"], inp["R"], inp["delta_b"], inp["delta_q"], inp["sampling_matrix"], inp["b0s_mask"])
+    assert BootDirectionGetter("CSA", 1.0, *args, fit="bf16x3").fit == "bf16x3"
+    assert BootDirectionGetter("CSA", 1.0, *args).fit == "fp32"
+    with pytest.raises(ValueError):
+        BootDirectionGetter("OPDT", 1.0, *args, fit="bf16x3")
+    with pytest.raises(ValueError):
+        BootDirectionGetter("CSA", 1.0, *args, fit="tf32")

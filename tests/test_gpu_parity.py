@@ -31,7 +31,7 @@ from conftest import ROOT
 pytestmark = pytest.mark.gpu
 
 
-def _handle(name, inp=None, seed_order=0):
+def _handle(name, inp=None, seed_order=0, boot_fit=0):
     from gpustreamlines_b200 import _lib
     from oracle import cases
 
@@ -51,6 +51,7 @@ def _handle(name, inp=None, seed_order=0):
     p.pmf_threshold = 0.05
     p.rng_seed = int(c["rng_seed"])
     p.seed_order = seed_order
+    p.boot_fit = boot_fit
     ins = _lib.CslInputs()
     ins.stop_map = _lib.fptr(inp["stop_map"])
     ins.vertices = _lib.fptr(inp["vertices"])
