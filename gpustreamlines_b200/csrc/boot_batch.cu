@@ -42,7 +42,8 @@
 namespace csl {
 
 constexpr int kSlots = 128;         // slots per CTA = MMA M = TMEM lanes
-constexpr int kBThreads = 128;      // one thread per slot, 4 warps
+constexpr int kBWarps = 16;
+constexpr int kBThreads = kBWarps * kWarp;
 constexpr int kBootAttempts = 5;    // bootstrap draws per step (boot.cu tracking)
 constexpr int kOdfChunk = 256;      // vertices per MMA-3 chunk (TMEM columns)
 constexpr int kTmemCols = 512;
@@ -65,11 +66,14 @@ BootBatchGeom boot_batch_geom(const DevParams &P, int hr, int nb0) {
     g.b1_chunk = 128 * g.N1;          // 2 terms x N1 rows x 32 k x 2 B
     g.b2_bytes = 4 * g.N2 * g.HP;     // 2 terms x N2 rows x HP k x 2 B
     g.b3_chunk = 1024 * g.N2;         // 2 terms x 256 rows x N2 k x 2 B
-    const int a1 = 512 * g.HP, rbuf = 512 * (hr + 1), a3 = 512 * g.N2, pk = 32 * g.vstride;
-    g.r0 = round_up(std::max(std::max(a1, rbuf), std::max(a3, pk)), 1024);
-    g.r1 = round_up(std::max(std::max(2 * g.b1_chunk, 512 * g.HP), g.b3_chunk), 1024);
+    const int a1 = 512 * g.HP, rbuf = 512 * (hr + 1), a3 = 512 * g.N2;
+    const int pk = kBWarps * 2 * g.vstride * 4;  // per-warp ODF + flag rows, spans R0 and R1
+    g.r0 = round_up(std::max(std::max(a1, rbuf), a3), 1024);
+    g.r1 = round_up(std::max(std::max(std::max(2 * g.b1_chunk, 512 * g.HP), g.b3_chunk), pk - g.r0), 1024);
     g.r2 = round_up(g.b2_bytes, 1024);
-    g.smem = 1024 + g.r0 + g.r1 + g.r2 + 4 * g.HP * 4 + kMaxSortLayers * kWarp * 4 + 128;
+    g.nbr_shorts = round_up(g.V * kMaxDegree, 8);
+    g.smem = 1024 + g.r0 + g.r1 + g.r2 + 3 * kSlots * 16 + 2 * kSlots * 4 + g.nbr_shorts * 2 +
+             kMaxSortLayers * kWarp * 4 + 128;
     return g;
 }
 
@@ -182,6 +186,37 @@ __device__ __forceinline__ void split8(const float (&x)[8], uint4 &hi, uint4 &lo
     lo = make_uint4(l[0], l[1], l[2], l[3]);
 }
 
+// Local-maximum flags from a per-vertex neighbour table instead of the edge
+// list with shared-memory atomics: flag -1 where some neighbour is larger, else
+// 1 where some neighbour is smaller, else 0 -- the values the edge loop of
+// peak_directions_d leaves (its -1 always wins over |= 1).  Unused table
+// entries hold the vertex itself, which compares neither larger nor smaller.
+__device__ __forceinline__ int peak_directions_nbr(const DevParams &P, const float *odf, int *ind, int nr,
+                                                   const short *__restrict__ nbr, const int *partner_sh,
+                                                   int lane) {
+    float mn = FLT_MAX;
+    for (int i = lane; i < nr; i += kWarp) mn = fmin_ref(mn, odf[i]);
+    float odf_min = warp_min_ref(mn);
+    odf_min = (0 > odf_min) ? 0 : odf_min;
+    for (int v = lane; v < nr; v += kWarp) {
+        const float x = odf[v];
+        bool larger = false, smaller = false;
+#pragma unroll
+        for (int d = 0; d < kMaxDegree; d++) {
+            const float y = odf[nbr[v * kMaxDegree + d]];
+            larger |= x < y;
+            smaller |= y < x;
+        }
+        ind[v] = larger ? -1 : (smaller ? 1 : 0);
+    }
+    __syncwarp();
+    return peak_select(P, odf, ind, nr, odf_min, partner_sh, lane);
+}
+
+// One CTA = 128 slots, 16 warps.  Warp w owns TMEM lane quadrant w % 4 for
+// the epilogues (the four warps of a quadrant split the columns) and slots
+// 8w .. 8w+7 for the warp-cooperative gather and peak search; threads
+// 0..127 own slot t's tracking state.
 __global__ void __launch_bounds__(kBThreads, 1)
     boot_batch_kernel(DevParams P, BootBatchGeom g, BootBatchArgs A, const int *partner) {
     extern __shared__ unsigned char smraw[];
@@ -190,14 +225,23 @@ __global__ void __launch_bounds__(kBThreads, 1)
     unsigned char *R0 = sm;
     unsigned char *R1 = R0 + g.r0;
     unsigned char *R2 = R1 + g.r1;
-    float *sig = reinterpret_cast<float *>(R2 + g.r2);
-    int *partner_sh = reinterpret_cast<int *>(sig + 4 * g.HP);
+    float4 *s_pt = reinterpret_cast<float4 *>(R2 + g.r2);   // [128] position, .w = b0 mean
+    float4 *s_dir = s_pt + kSlots;                           // [128] incoming direction
+    float4 *s_new = s_dir + kSlots;                          // [128] new direction, .w = found
+    int *s_h = reinterpret_cast<int *>(s_new + kSlots);      // [128] half id, -1 = empty
+    int *s_live = s_h + kSlots;                              // [128] attempt this iteration
+    short *nbr_sh = reinterpret_cast<short *>(s_live + kSlots);  // [V][kMaxDegree]
+    int *partner_sh = reinterpret_cast<int *>(nbr_sh + g.nbr_shorts);
     uint64_t *bars = reinterpret_cast<uint64_t *>(partner_sh + kMaxSortLayers * kWarp);
     // bars: 0, 1 = B1 stage loaded; 2, 3 = B1 stage consumed; 4 = MMA batch done; 5 = B2/B3 loaded
     uint32_t *tmem_sh = reinterpret_cast<uint32_t *>(bars + 6);
 
     const int t = threadIdx.x, w = t >> 5, lane = t & 31;
+    const int qd = w & 3, part = w >> 2;        // epilogue: lane quadrant, column share
+    const int eslot = qd * 32 + lane;           // epilogue slot of this thread
     for (int i = t; i < kMaxSortLayers * kWarp; i += kBThreads) partner_sh[i] = partner[i];
+    for (int i = t; i < g.V * kMaxDegree; i += kBThreads) nbr_sh[i] = A.nbr[i];
+    if (t < kSlots) s_h[t] = -1;
     if (t == 0) {
         for (int b = 0; b < 6; b++) mbar_init(&bars[b], 1);
         mbar_fence_init();
@@ -207,7 +251,7 @@ __global__ void __launch_bounds__(kBThreads, 1)
     __syncthreads();
     tc_fence_after();
     const uint32_t tbase = *tmem_sh;
-    const uint32_t trow = tbase + ((uint32_t)(w * 32) << 16);
+    const uint32_t trow = tbase + ((uint32_t)(qd * 32) << 16);
 
     uint32_t ph_load[2] = {0, 0}, ph_free[2] = {0, 0}, ph_mma = 0, ph_aux = 0;
     bool ok = true;
@@ -224,44 +268,45 @@ __global__ void __launch_bounds__(kBThreads, 1)
     const uint32_t a1_term = 256 * g.HP, a3_term = 256 * g.N2;
     const uint32_t b1_term = g.b1_chunk / 2, b2_term = g.b2_bytes / 2, b3_term = g.b3_chunk / 2;
     const int imax = P.max_sline_len;
-    const int T = P.dimt;
-    const int slot_g = blockIdx.x * kSlots + t;
-    float *my_pts = A.pts + (size_t)slot_g * (size_t)imax * 3;
-    float *my_odf = A.odf + (size_t)slot_g * g.vstride;
 
+    // tracking state of slot t (threads 0..127)
     int my_h = -1, my_i = 0, my_att = 0;
     float3 my_pt = make_float3(0, 0, 0), my_dir = make_float3(0, 0, 0);
-    bool my_valid = false, queue_empty = false;
-    float my_denom = 1.0f;
+    bool queue_empty = false;
+    // bootstrap stream of (epilogue slot, column share)
     Philox rng;
     rng.init(0, 0, 0);
+    int rng_h = -1;
 
     for (;;) {
         // ---- refill empty slots from the queue of streamline halves
-        if (my_h < 0 && !queue_empty) {
-            const int h = atomicAdd(A.hq, 1);
-            if (h >= 2 * A.nsl) {
-                queue_empty = true;
-            } else {
-                my_h = h;
-                const int sl = h >> 1, half = h & 1;
-                const int s = A.sl_seed[sl];
-                const float3 v = vert3(P.verts, (int)A.sl_vert[sl]);
-                my_pt = make_float3(A.seeds[3 * s], A.seeds[3 * s + 1], A.seeds[3 * s + 2]);
-                my_dir = half ? v : make_float3(-v.x, -v.y, -v.z);
-                my_i = 1;
-                my_att = 0;
-                rng.init(P.rng_seed, kBatchSubseqBase + 2ull * (unsigned long long)(sl + A.rng_base) + half,
-                         0);
-                store_pt(my_pts, 0, my_pt);
+        if (t < kSlots) {
+            if (my_h < 0 && !queue_empty) {
+                const int h = atomicAdd(A.hq, 1);
+                if (h >= 2 * A.nsl) {
+                    queue_empty = true;
+                } else {
+                    my_h = h;
+                    const int sl = h >> 1, half = h & 1;
+                    const int s = A.sl_seed[sl];
+                    const float3 v = vert3(P.verts, (int)A.sl_vert[sl]);
+                    my_pt = make_float3(A.seeds[3 * s], A.seeds[3 * s + 1], A.seeds[3 * s + 2]);
+                    my_dir = half ? v : make_float3(-v.x, -v.y, -v.z);
+                    my_i = 1;
+                    my_att = 0;
+                    store_pt(A.pts + ((size_t)blockIdx.x * kSlots + t) * (size_t)imax * 3, 0, my_pt);
+                }
             }
+            s_h[t] = my_h;
+            s_live[t] = (my_h >= 0) && (my_i < imax);
+            s_pt[t] = make_float4(my_pt.x, my_pt.y, my_pt.z, 1.0f);
+            s_dir[t] = make_float4(my_dir.x, my_dir.y, my_dir.z, 0.0f);
         }
         if (__syncthreads_or(!ok)) {
             if (t == 0) atomicOr(A.status, ST_WAIT_TIMEOUT);
             break;
         }
-        if (!__syncthreads_or(my_h >= 0)) break;
-        const bool attempt = (my_h >= 0) && (my_i < imax);
+        if (!__syncthreads_or(t < kSlots && my_h >= 0)) break;
 
         // ---- B1 stages 0 and 1 (R1 is free: the last iteration's MMAs are done)
         if (t == 0) {
@@ -271,54 +316,41 @@ __global__ void __launch_bounds__(kBThreads, 1)
             }
         }
 
-        // ---- gather: the warp interpolates its 32 slots' signals into A1 rows
-        {
-            float *sg = sig + w * g.HP;
-            const unsigned am = __ballot_sync(FULL, attempt);
-            bool vmine = false;
-            float dmine = 1.0f;
-            for (int i = 0; i < kWarp; i++) {
-                const int slot = w * 32 + i;
-                const float3 p = make_float3(__shfl_sync(FULL, my_pt.x, i), __shfl_sync(FULL, my_pt.y, i),
-                                             __shfl_sync(FULL, my_pt.z, i));
-                Corners c;
-                bool inb = false;
-                if ((am >> i) & 1u) inb = trilinear_setup(P, p, c);
-                float bsum = 0.0f;
-                if (inb) {
-                    for (int tt = lane; tt < T; tt += kWarp) {
-                        const float v = trilinear_elem(P.dataf, c, tt);
-                        const int k = __ldg(A.nbpos + tt);
-                        if (k >= 0)
-                            sg[k] = v;
-                        else
-                            bsum += (P.min_signal > v) ? P.min_signal : v;
-                    }
-                }
+        // ---- gather: warp w interpolates slots 8w..8w+7 into A1 rows; lane l
+        //      builds k = 8l .. 8l+7 of the non-b0 signal, lanes past the
+        //      non-b0 groups add up the clamped b0 values
+        for (int i = 0; i < kSlots / kBWarps; i++) {
+            const int slot = w * (kSlots / kBWarps) + i;
+            const float4 p4 = s_pt[slot];
+            Corners c;
+            bool inb = false;
+            if (s_live[slot]) inb = trilinear_setup(P, make_float3(p4.x, p4.y, p4.z), c);
+            const int ng = g.HP / 8;
+            float bsum = 0.0f;
+            if (lane < ng) {
+                float x[8];
 #pragma unroll
-                for (int o = 16; o; o >>= 1) bsum += __shfl_xor_sync(FULL, bsum, o);
-                __syncwarp();
-                for (int gq = lane; gq < g.HP / 8; gq += kWarp) {
-                    float x[8];
-#pragma unroll
-                    for (int e = 0; e < 8; e++) {
-                        const int k = gq * 8 + e;
-                        x[e] = (inb && k < g.hr) ? sg[k] : 0.0f;
-                    }
-                    uint4 hi, lo;
-                    split8(x, hi, lo);
-                    const uint32_t off = kmajor_off(slot, gq * 8, kSlots);
-                    *reinterpret_cast<uint4 *>(R0 + off) = hi;
-                    *reinterpret_cast<uint4 *>(R0 + a1_term + off) = lo;
+                for (int e = 0; e < 8; e++) {
+                    const int k = lane * 8 + e;
+                    x[e] = (inb && k < g.hr) ? trilinear_elem(P.dataf, c, __ldg(A.volidx + k)) : 0.0f;
                 }
-                __syncwarp();
-                if (lane == i) {
-                    vmine = inb;
-                    dmine = bsum / (float)g.nb0;
+                uint4 hi, lo;
+                split8(x, hi, lo);
+                const uint32_t off = kmajor_off(slot, lane * 8, kSlots);
+                *reinterpret_cast<uint4 *>(R0 + off) = hi;
+                *reinterpret_cast<uint4 *>(R0 + a1_term + off) = lo;
+            } else if (inb) {
+                for (int b = lane - ng; b < g.nb0; b += kWarp - ng) {
+                    const float v = trilinear_elem(P.dataf, c, __ldg(A.volidx + g.hr + b));
+                    bsum += (P.min_signal > v) ? P.min_signal : v;
                 }
             }
-            my_valid = vmine;
-            my_denom = dmine;
+#pragma unroll
+            for (int o = 16; o; o >>= 1) bsum += __shfl_xor_sync(FULL, bsum, o);
+            if (lane == 0) {
+                s_pt[slot].w = bsum / (float)g.nb0;
+                s_live[slot] = inb ? 1 : 0;  // outside the data: every attempt would fail
+            }
         }
         fence_async_smem();
         __syncthreads();
@@ -364,32 +396,43 @@ __global__ void __launch_bounds__(kBThreads, 1)
         ph_mma ^= 1;
         tc_fence_after();
 
-        // ---- epilogue 1: residuals to shared memory, bootstrap, CSA transform -> A2
-        {
-            float *rb = reinterpret_cast<float *>(R0) + (size_t)t * (g.hr + 1);
-            for (int c0 = 0; c0 < g.HP; c0 += 16) {
-                float v[16];
-                tmem_ld16(trow + c0, v);
+        // ---- epilogue 1: residuals to shared memory (this thread's column
+        //      blocks), then bootstrap, clamp, normalise, CSA transform -> A2
+        float *rb = reinterpret_cast<float *>(R0) + (size_t)eslot * (g.hr + 1);
+        const int nblk1 = g.HP / 16;
+        for (int b = part; b < nblk1; b += 4) {
+            float v[16];
+            tmem_ld16(trow + 16 * b, v);
 #pragma unroll
-                for (int q = 0; q < 16; q++)
-                    if (c0 + q < g.hr) rb[c0 + q] = v[q];
+            for (int q = 0; q < 16; q++)
+                if (16 * b + q < g.hr) rb[16 * b + q] = v[q];
+        }
+        __syncthreads();
+        {
+            const int h = s_h[eslot];
+            const bool live = s_live[eslot] != 0;
+            const float denom = s_pt[eslot].w;
+            if (live && h != rng_h) {
+                const int sl = h >> 1, half = h & 1;
+                rng.init(P.rng_seed,
+                         kBatchSubseqBase + 8ull * (unsigned long long)(sl + A.rng_base) + 4 * half + part, 0);
+                rng_h = h;
             }
-            const bool live = attempt && my_valid;
-            for (int c0 = 0; c0 < g.HP; c0 += 16) {
+            for (int b = part; b < nblk1; b += 4) {
                 float hv[16];
-                tmem_ld16(trow + g.HP + c0, hv);
+                tmem_ld16(trow + g.HP + 16 * b, hv);
 #pragma unroll
                 for (int gq = 0; gq < 2; gq++) {
                     float y[8];
 #pragma unroll
                     for (int e = 0; e < 8; e++) {
-                        const int j = c0 + gq * 8 + e;
+                        const int j = 16 * b + gq * 8 + e;
                         y[e] = 0.0f;
                         if (live && j < g.hr) {
                             const int src = (int)(rng.next() % (unsigned)g.hr);
                             float x = hv[gq * 8 + e] + rb[src];
                             x = (P.min_signal > x) ? P.min_signal : x;
-                            x = x / my_denom;
+                            x = x / denom;
                             const float lo_c = 0.001f, hi_c = 0.999f;
                             float cc = (x > lo_c) ? x : lo_c;
                             cc = (cc < hi_c) ? cc : hi_c;
@@ -398,7 +441,7 @@ __global__ void __launch_bounds__(kBThreads, 1)
                     }
                     uint4 hi, lo;
                     split8(y, hi, lo);
-                    const uint32_t off = kmajor_off(t, c0 + gq * 8, kSlots);
+                    const uint32_t off = kmajor_off(eslot, 16 * b + gq * 8, kSlots);
                     *reinterpret_cast<uint4 *>(R1 + off) = hi;
                     *reinterpret_cast<uint4 *>(R1 + a1_term + off) = lo;
                 }
@@ -428,20 +471,20 @@ __global__ void __launch_bounds__(kBThreads, 1)
         tc_fence_after();
 
         // ---- epilogue 2: SH coefficients -> A3 (coefficient 0 fixed, boot.cu CSA branch)
-        for (int c0 = 0; c0 < g.N2; c0 += 16) {
+        for (int b = part; b < g.N2 / 16; b += 4) {
             float v[16];
-            tmem_ld16(trow + g.N1 + c0, v);
+            tmem_ld16(trow + g.N1 + 16 * b, v);
 #pragma unroll
             for (int gq = 0; gq < 2; gq++) {
                 float x[8];
 #pragma unroll
                 for (int e = 0; e < 8; e++) {
-                    const int k = c0 + gq * 8 + e;
+                    const int k = 16 * b + gq * 8 + e;
                     x[e] = (k == 0) ? kN0Const : (k < g.C ? v[gq * 8 + e] : 0.0f);
                 }
                 uint4 hi, lo;
                 split8(x, hi, lo);
-                const uint32_t off = kmajor_off(t, c0 + gq * 8, kSlots);
+                const uint32_t off = kmajor_off(eslot, 16 * b + gq * 8, kSlots);
                 *reinterpret_cast<uint4 *>(R0 + off) = hi;
                 *reinterpret_cast<uint4 *>(R0 + a3_term + off) = lo;
             }
@@ -451,6 +494,7 @@ __global__ void __launch_bounds__(kBThreads, 1)
         __syncthreads();
 
         // ---- MMA 3 in 256-vertex chunks: ODF rows -> L2 scratch
+        float *e_odf = A.odf + ((size_t)blockIdx.x * kSlots + eslot) * g.vstride;
         for (int ch = 0; ch < g.nchunk3; ch++) {
             if (t == 0 && ok) {
                 mbar_arrive_expect_tx(&bars[5], (uint32_t)g.b3_chunk);
@@ -477,112 +521,113 @@ __global__ void __launch_bounds__(kBThreads, 1)
             if (!mbar_wait(&bars[4], ph_mma)) ok = false;
             ph_mma ^= 1;
             tc_fence_after();
-            for (int c0 = 0; c0 < kOdfChunk; c0 += 16) {
+            for (int b = part; b < kOdfChunk / 16; b += 4) {
                 float v[16];
-                tmem_ld16(trow + c0, v);
-                const int vb = ch * kOdfChunk + c0;
+                tmem_ld16(trow + 16 * b, v);
+                const int vb = ch * kOdfChunk + 16 * b;
                 if (vb + 16 <= g.V) {
 #pragma unroll
                     for (int q = 0; q < 16; q += 4)
-                        __stcg(reinterpret_cast<float4 *>(my_odf + vb + q),
+                        __stcg(reinterpret_cast<float4 *>(e_odf + vb + q),
                                make_float4(v[q], v[q + 1], v[q + 2], v[q + 3]));
                 } else {
 #pragma unroll
                     for (int q = 0; q < 16; q++)
-                        if (vb + q < g.V) my_odf[vb + q] = v[q];
+                        if (vb + q < g.V) e_odf[vb + q] = v[q];
                 }
             }
             tc_fence_before();
             __syncthreads();
         }
 
-        // ---- peaks and closest peak: one warp per slot, the plain getter's code
-        bool my_found = false;
-        float3 my_new = make_float3(0, 0, 0);
+        // ---- peaks and closest peak: warp w searches slots 8w..8w+7
         {
             float *odf_sh = reinterpret_cast<float *>(R0) + (size_t)w * 2 * g.vstride;
             int *ind_sh = reinterpret_cast<int *>(odf_sh + g.vstride);
-            const unsigned am = __ballot_sync(FULL, attempt && my_valid);
-            for (int i = 0; i < kWarp; i++) {
-                if (!((am >> i) & 1u)) continue;
-                const float *src = A.odf + ((size_t)blockIdx.x * kSlots + w * 32 + i) * g.vstride;
-                for (int v = lane; v < g.V; v += kWarp) odf_sh[v] = __ldcg(src + v);
-                __syncwarp();
-                const float3 di = make_float3(__shfl_sync(FULL, my_dir.x, i), __shfl_sync(FULL, my_dir.y, i),
-                                              __shfl_sync(FULL, my_dir.z, i));
+            for (int i = 0; i < kSlots / kBWarps; i++) {
+                const int slot = w * (kSlots / kBWarps) + i;
+                if (!s_live[slot]) continue;
+                const float *src = A.odf + ((size_t)blockIdx.x * kSlots + slot) * g.vstride;
                 float m = -FLT_MAX;
-                for (int v = lane; v < g.V; v += kWarp) m = fmax_ref(m, odf_sh[v]);
+                for (int v = lane; v < g.V; v += kWarp) {
+                    const float x = __ldcg(src + v);
+                    odf_sh[v] = x;
+                    m = fmax_ref(m, x);
+                }
                 m = warp_max_ref(m);
                 const float thr = (float)(P.pmf_threshold * (double)m);
-                __syncwarp();
                 for (int v = lane; v < g.V; v += kWarp)
                     if (odf_sh[v] < thr) odf_sh[v] = 0;
                 __syncwarp();
-                const int ndir = peak_directions(P, odf_sh, ind_sh, g.V, partner_sh, lane);
+                const int ndir = peak_directions_nbr(P, odf_sh, ind_sh, g.V, nbr_sh, partner_sh, lane);
                 int found = 0;
                 float3 pk = make_float3(0, 0, 0);
-                if (ndir > 0) found = closest_peak(P, di, ndir, ind_sh, lane, &pk);
-                __syncwarp();
-                if (lane == i) {
-                    my_found = found != 0;
-                    my_new = pk;
+                if (ndir > 0) {
+                    const float4 d4 = s_dir[slot];
+                    found = closest_peak(P, make_float3(d4.x, d4.y, d4.z), ndir, ind_sh, lane, &pk);
                 }
+                __syncwarp();
+                if (lane == 0) s_new[slot] = make_float4(pk.x, pk.y, pk.z, found ? 1.0f : 0.0f);
             }
         }
+        __syncthreads();
 
         // ---- step (tracker_boot_d, boot.cu:725-824): one attempt per iteration
-        bool done = false;
-        int nsteps = 0;
-        if (my_h >= 0) {
-            if (!attempt || !my_valid) {
-                done = true;  // no step left, or outside the data: every attempt would fail
-                nsteps = my_i;
-            } else if (my_found) {
-                my_dir = my_new;
-                const double ss = P.step_size;
-                my_pt.x = (float)fma((double)my_dir.x, ss, (double)my_pt.x);
-                my_pt.y = (float)fma((double)my_dir.y, ss, (double)my_pt.y);
-                my_pt.z = (float)fma((double)my_dir.z, ss, (double)my_pt.z);
-                store_pt(my_pts, my_i, my_pt);
-                my_att = 0;
-                if (check_point(P, my_pt) != TRACKPOINT) {
-                    done = true;
+        if (w < kSlots / kWarp) {
+            bool done = false;
+            int nsteps = 0;
+            if (my_h >= 0) {
+                const float4 nw = s_new[t];
+                if (!s_live[t]) {
+                    done = true;  // no step left, or outside the data: every attempt would fail
                     nsteps = my_i;
-                } else if (++my_i >= imax) {
+                } else if (nw.w != 0.0f) {
+                    my_dir = make_float3(nw.x, nw.y, nw.z);
+                    const double ss = P.step_size;
+                    my_pt.x = (float)fma((double)my_dir.x, ss, (double)my_pt.x);
+                    my_pt.y = (float)fma((double)my_dir.y, ss, (double)my_pt.y);
+                    my_pt.z = (float)fma((double)my_dir.z, ss, (double)my_pt.z);
+                    store_pt(A.pts + ((size_t)blockIdx.x * kSlots + t) * (size_t)imax * 3, my_i, my_pt);
+                    my_att = 0;
+                    if (check_point(P, my_pt) != TRACKPOINT) {
+                        done = true;
+                        nsteps = my_i;
+                    } else if (++my_i >= imax) {
+                        done = true;
+                        nsteps = my_i;
+                    }
+                } else if (++my_att >= kBootAttempts) {
                     done = true;
                     nsteps = my_i;
                 }
-            } else if (++my_att >= kBootAttempts) {
-                done = true;
-                nsteps = my_i;
             }
-        }
 
-        // ---- finished halves: append their points to the pool
-        __syncwarp();
-        unsigned dm = __ballot_sync(FULL, done);
-        while (dm) {
-            const int i = __ffs(dm) - 1;
-            dm &= dm - 1;
-            const int n = __shfl_sync(FULL, nsteps, i);
-            const int h = __shfl_sync(FULL, my_h, i);
-            const float *src = A.pts + ((size_t)blockIdx.x * kSlots + w * 32 + i) * (size_t)imax * 3;
-            unsigned long long off = 0;
-            if (lane == 0) off = atomicAdd(A.pool_count, (unsigned long long)n);
-            off = __shfl_sync(FULL, off, 0);
-            long long o = -1;
-            if (off + (unsigned long long)n <= A.pool_cap) {
-                o = (long long)off;
-                for (int j = lane; j < 3 * n; j += kWarp) A.pool[3 * off + j] = __ldcg(src + j);
-            } else if (lane == 0) {
-                atomicOr(A.status, ST_POOL_OVERFLOW);
+            // finished halves: append their points to the pool
+            __syncwarp();
+            unsigned dm = __ballot_sync(FULL, done);
+            while (dm) {
+                const int i = __ffs(dm) - 1;
+                dm &= dm - 1;
+                const int n = __shfl_sync(FULL, nsteps, i);
+                const int h = __shfl_sync(FULL, my_h, i);
+                const float *src = A.pts + ((size_t)blockIdx.x * kSlots + w * 32 + i) * (size_t)imax * 3;
+                unsigned long long off = 0;
+                if (lane == 0) off = atomicAdd(A.pool_count, (unsigned long long)n);
+                off = __shfl_sync(FULL, off, 0);
+                long long o = -1;
+                if (off + (unsigned long long)n <= A.pool_cap) {
+                    o = (long long)off;
+                    for (int j = lane; j < 3 * n; j += kWarp) A.pool[3 * off + j] = __ldcg(src + j);
+                } else if (lane == 0) {
+                    atomicOr(A.status, ST_POOL_OVERFLOW);
+                }
+                if (lane == 0) {
+                    A.half_len[h] = n;
+                    A.half_off[h] = o;
+                }
             }
-            if (lane == 0) {
-                A.half_len[h] = n;
-                A.half_off[h] = o;
-            }
+            if (done) my_h = -1;
         }
-        if (done) my_h = -1;
     }
 
     // ---- teardown: every MMA has completed (each batch was waited for)

@@ -80,7 +80,8 @@ struct csl_tracker {
     // batched bootstrap fit (boot_fit == 1)
     BootBatchGeom bgeom{};
     DevBuf<unsigned char> bb_B1, bb_B2, bb_B3;
-    DevBuf<int> bb_nbpos, bb_sl_seed, bb_half_len, bb_hq;
+    DevBuf<int> bb_volidx, bb_sl_seed, bb_half_len, bb_hq;
+    DevBuf<short> bb_nbr;
     DevBuf<short> bb_sl_vert;
     DevBuf<long long> bb_half_off;
     DevBuf<float> bb_odf, bb_pts;
@@ -231,13 +232,14 @@ static void release_all(csl_tracker *t) {
     t->sort_tmp.release();
     t->mkeys.release();
     t->mkeys_sorted.release();
-    DevBuf<int> *ib2[] = {&t->mvals, &t->perm, &t->blk_next, &t->blk_end, &t->bb_nbpos,
+    DevBuf<int> *ib2[] = {&t->mvals, &t->perm, &t->blk_next, &t->blk_end, &t->bb_volidx,
                           &t->bb_sl_seed, &t->bb_half_len, &t->bb_hq};
     for (auto *b : ib2) b->release();
     t->bb_B1.release();
     t->bb_B2.release();
     t->bb_B3.release();
     t->bb_sl_vert.release();
+    t->bb_nbr.release();
     t->bb_half_off.release();
     t->bb_odf.release();
     t->bb_pts.release();
@@ -407,12 +409,39 @@ int csl_create(const csl_params *params, const csl_inputs *inputs, int device, c
             if (p.boot_fit == 1) {
                 if (hr > 160)
                     return fail(t, CSL_E_INVALID, "boot_fit=1 supports at most 160 non-b0 volumes, got %d", hr);
-                std::vector<int> nbpos(p.dimt);
-                int k = 0;
-                for (int i = 0; i < p.dimt; i++) nbpos[i] = inputs->b0s_mask[i] ? -1 : k++;
+                // volume order of the batched gather: non-b0 volumes, then b0s
+                std::vector<int> volidx;
+                for (int i = 0; i < p.dimt; i++)
+                    if (!inputs->b0s_mask[i]) volidx.push_back(i);
+                for (int i = 0; i < p.dimt; i++)
+                    if (inputs->b0s_mask[i]) volidx.push_back(i);
+                // sphere neighbour table for the batched peak search
+                std::vector<short> nbr((size_t)p.nvertices * kMaxDegree);
+                std::vector<int> deg(p.nvertices, 0);
+                for (int v = 0; v < p.nvertices; v++)
+                    for (int d = 0; d < kMaxDegree; d++) nbr[(size_t)v * kMaxDegree + d] = (short)v;
+                for (int e = 0; e < p.nedges; e++) {
+                    const int a = inputs->edges[2 * e], b = inputs->edges[2 * e + 1];
+                    if (a < 0 || b < 0 || a >= p.nvertices || b >= p.nvertices)
+                        return fail(t, CSL_E_INVALID, "edge %d references a missing vertex", e);
+                    const int ab[2][2] = {{a, b}, {b, a}};
+                    for (const auto &q : ab) {
+                        bool seen = false;
+                        for (int d = 0; d < deg[q[0]]; d++) seen |= nbr[(size_t)q[0] * kMaxDegree + d] == q[1];
+                        if (seen) continue;
+                        if (deg[q[0]] == kMaxDegree)
+                            return fail(t, CSL_E_INVALID, "boot_fit=1 supports spheres of vertex degree <= %d",
+                                        kMaxDegree);
+                        nbr[(size_t)q[0] * kMaxDegree + deg[q[0]]++] = (short)q[1];
+                    }
+                }
                 const BootBatchGeom g = boot_batch_geom(P, hr, p.dimt - hr);
                 t->bgeom = g;
-                if ((r = upload(t, t->bb_nbpos, nbpos.data(), nbpos.size()))) return r;
+                if (g.smem > 227 * 1024)
+                    return fail(t, CSL_E_INVALID, "boot_fit=1 needs %d B of shared memory per block", g.smem);
+                if ((r = upload(t, t->bb_volidx, volidx.data(), volidx.size()))) return r;
+                nbr.resize((size_t)g.nbr_shorts, 0);
+                if ((r = upload(t, t->bb_nbr, nbr.data(), nbr.size()))) return r;
                 CK(t->bb_B1.ensure((size_t)g.nchunk1 * g.b1_chunk));
                 CK(t->bb_B2.ensure((size_t)g.b2_bytes));
                 CK(t->bb_B3.ensure((size_t)g.nchunk3 * g.b3_chunk));
@@ -515,7 +544,8 @@ static int run_boot_batch(csl_tracker *t, const float *seeds_dev, int ni, int ns
         A.B1g = t->bb_B1.p;
         A.B2g = t->bb_B2.p;
         A.B3g = t->bb_B3.p;
-        A.nbpos = t->bb_nbpos.p;
+        A.volidx = t->bb_volidx.p;
+        A.nbr = t->bb_nbr.p;
         A.seeds = seeds_dev;
         A.sl_seed = t->bb_sl_seed.p;
         A.sl_vert = t->bb_sl_vert.p;

@@ -214,9 +214,11 @@ __device__ __forceinline__ float3 vert3(const float *__restrict__ verts, int i) 
 // `odf` and `ind` are per-warp shared arrays of length >= nr.  On return
 // ind[0..n) hold the kept peak vertex indices in reference order.
 
+__device__ __forceinline__ int peak_select(const DevParams &P, const float *odf, int *ind, int nr,
+                                           float odf_min, const int *__restrict__ partner_sh, int lane);
+
 __device__ __forceinline__ int peak_directions(const DevParams &P, const float *odf, int *ind, int nr,
                                const int *__restrict__ partner_sh, int lane) {
-    const unsigned lmask = (1u << lane) - 1u;
     for (int j = lane; j < nr; j += kWarp) ind[j] = 0;
 
     float mn = FLT_MAX;
@@ -240,6 +242,15 @@ __device__ __forceinline__ int peak_directions(const DevParams &P, const float *
     }
     __syncwarp();
 
+    return peak_select(P, odf, ind, nr, odf_min, partner_sh, lane);
+}
+
+// The part of peak_directions_d after the local-maximum flags are in ind[]
+// (1 = local maximum, tracking_helpers.cu:163-244): relative threshold over the
+// maxima, compaction, descending sort, minimum-separation filter.
+__device__ __forceinline__ int peak_select(const DevParams &P, const float *odf, int *ind, int nr,
+                                           float odf_min, const int *__restrict__ partner_sh, int lane) {
+    const unsigned lmask = (1u << lane) - 1u;
     // RELATIVE_PEAK_THRESH * max over maxima of (odf + (-odf_min))
     float mm = -FLT_MAX;
     const float neg_min = -odf_min;

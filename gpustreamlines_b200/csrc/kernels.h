@@ -38,6 +38,8 @@ cudaError_t launch_philox_stream(unsigned long long seed, unsigned long long sub
                                  unsigned long long offset, long long n, unsigned *out,
                                  cudaStream_t st);
 // ---- batched bootstrap fit on the tensor cores (boot_batch.cu)
+constexpr int kMaxDegree = 8;  // neighbour-table width of the batched peak search
+
 struct BootBatchGeom {
     int hr, nb0;        // non-b0 / b0 volumes
     int HP, N1;         // hr padded to 32; rows of [R ; H] = 2 HP
@@ -45,13 +47,15 @@ struct BootBatchGeom {
     int V, nchunk1, nchunk3, vstride;
     int b1_chunk, b2_bytes, b3_chunk;  // bytes of one packed operand chunk (hi + lo)
     int r0, r1, r2, smem;              // shared-memory regions and total
+    int nbr_shorts;                    // V * kMaxDegree, padded to 16 bytes
 };
 
 struct BootBatchArgs {
     const unsigned char *B1g;  // [HP/32][2][2HP x 32] packed [R ; H]
     const unsigned char *B2g;  // [2][N2 x HP] packed delta_q
     const unsigned char *B3g;  // [nchunk3][2][256 x N2] packed sampling matrix
-    const int *nbpos;          // [T] index among the non-b0 volumes, -1 for a b0
+    const int *volidx;         // [T] volume indices: the hr non-b0 volumes, then the b0s
+    const short *nbr;          // [V][kMaxDegree] sphere neighbours, padded with the vertex itself
     const float *seeds;
     const int *sl_seed;        // streamline -> seed (batch-local)
     const short *sl_vert;      // streamline -> initial vertex
