@@ -63,11 +63,12 @@ BootBatchGeom boot_batch_geom(const DevParams &P, int hr, int nb0) {
     g.nchunk1 = g.HP / 32;
     g.nchunk3 = (P.samplm_nr + kOdfChunk - 1) / kOdfChunk;
     g.vstride = round_up(P.samplm_nr, 4);
+    g.TP = round_up(P.dimt, 4);
     g.b1_chunk = 128 * g.N1;          // 2 terms x N1 rows x 32 k x 2 B
     g.b2_bytes = 4 * g.N2 * g.HP;     // 2 terms x N2 rows x HP k x 2 B
     g.b3_chunk = 1024 * g.N2;         // 2 terms x 256 rows x N2 k x 2 B
     const int a1 = 512 * g.HP, rbuf = 512 * (hr + 1), a3 = 512 * g.N2;
-    const int pk = kBWarps * 2 * g.vstride * 4;  // per-warp ODF + flag rows, spans R0 and R1
+    const int pk = kBWarps * 3 * g.vstride * 4;  // per-warp 2 ODF rows + flags, spans R0 and R1
     g.r0 = round_up(std::max(std::max(a1, rbuf), a3), 1024);
     g.r1 = round_up(std::max(std::max(std::max(2 * g.b1_chunk, 512 * g.HP), g.b3_chunk), pk - g.r0), 1024);
     g.r2 = round_up(g.b2_bytes, 1024);
@@ -119,6 +120,19 @@ __global__ void boot_batch_pack_kernel(DevParams P, BootBatchGeom g, __nv_bfloat
         const __nv_bfloat16 l = __float2bfloat16_rn(x - __bfloat162float(h));
         *reinterpret_cast<__nv_bfloat16 *>(hi + off) = h;
         *reinterpret_cast<__nv_bfloat16 *>(lo + off) = l;
+    }
+}
+
+// DWI copy for the batched gather: T axis reordered by volidx (non-b0 volumes
+// first, then the b0s) and padded to TP so every voxel row is 16-byte aligned
+__global__ void boot_batch_dwi_kernel(const float *__restrict__ src, const int *__restrict__ volidx,
+                                      long long nvox, int T, int TP, float *__restrict__ dst) {
+    const long long n = nvox * TP;
+    for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < n;
+         e += (long long)gridDim.x * blockDim.x) {
+        const long long vox = e / TP;
+        const int k = (int)(e - vox * TP);
+        dst[e] = k < T ? src[vox * T + volidx[k]] : 0.0f;
     }
 }
 
@@ -186,32 +200,145 @@ __device__ __forceinline__ void split8(const float (&x)[8], uint4 &hi, uint4 &lo
     lo = make_uint4(l[0], l[1], l[2], l[3]);
 }
 
-// Local-maximum flags from a per-vertex neighbour table instead of the edge
-// list with shared-memory atomics: flag -1 where some neighbour is larger, else
-// 1 where some neighbour is smaller, else 0 -- the values the edge loop of
-// peak_directions_d leaves (its -1 always wins over |= 1).  Unused table
-// entries hold the vertex itself, which compares neither larger nor smaller.
-__device__ __forceinline__ int peak_directions_nbr(const DevParams &P, const float *odf, int *ind, int nr,
-                                                   const short *__restrict__ nbr, const int *partner_sh,
-                                                   int lane) {
+// Peak search of one thresholded ODF row, warp-cooperative, with the
+// semantics of peak_directions_d (tracking_helpers.cu:75-245) and fewer
+// instructions:
+//  * only vertices that can be maxima are tested: after the 5 % threshold all
+//    values are >= 0 when the row maximum is positive, so a zero vertex has no
+//    smaller neighbour and is never a maximum;
+//  * a vertex is a maximum when no neighbour is larger and some neighbour is
+//    smaller -- the flag the edge loop with atomics leaves (its -1 wins over
+//    |= 1); neighbours come from a per-vertex table (unused entries hold the
+//    vertex itself, which is neither larger nor smaller);
+//  * maxima are kept in ascending vertex order, so the relative threshold,
+//    the descending sort network and its tie order are those of the reference;
+//  * the minimum-separation filter runs the reference's greedy loop with the
+//    inner scan over the kept peaks done by all lanes at once.
+// cand[] and ind[] may alias.  Returns the number of kept peaks, in ind[].
+__device__ __forceinline__ int peaks_sparse(const DevParams &P, float *odf, int *ind, int nr, float m,
+                                            const short *__restrict__ nbr, const int *partner_sh, int lane) {
+    const unsigned lmask = (1u << lane) - 1u;
+    const float thr = (float)(P.pmf_threshold * (double)m);
+    const bool all_cand = !(m > 0.0f);
+    // threshold in place, row minimum, candidate list (ascending)
     float mn = FLT_MAX;
-    for (int i = lane; i < nr; i += kWarp) mn = fmin_ref(mn, odf[i]);
+    int nc = 0;
+    for (int j = 0; j < nr; j += kWarp) {
+        const int v = j + lane;
+        bool c = false;
+        if (v < nr) {
+            float x = odf[v];
+            if (x < thr) {
+                x = 0;
+                odf[v] = 0;
+            }
+            mn = fmin_ref(mn, x);
+            c = all_cand || x > 0.0f;
+        }
+        const unsigned msk = __ballot_sync(FULL, c);
+        if (c) ind[nc + __popc(msk & lmask)] = v;
+        nc += __popc(msk);
+    }
     float odf_min = warp_min_ref(mn);
     odf_min = (0 > odf_min) ? 0 : odf_min;
-    for (int v = lane; v < nr; v += kWarp) {
-        const float x = odf[v];
-        bool larger = false, smaller = false;
+    __syncwarp();
+    // local maxima among the candidates, compacted in place (ascending)
+    int nm = 0;
+    for (int c0 = 0; c0 < nc; c0 += kWarp) {
+        bool mx = false;
+        int v = 0;
+        if (c0 + lane < nc) {
+            v = ind[c0 + lane];
+            const float x = odf[v];
+            const uint4 nb = *reinterpret_cast<const uint4 *>(nbr + v * kMaxDegree);
+            const uint32_t w4[4] = {nb.x, nb.y, nb.z, nb.w};
+            bool larger = false, smaller = false;
 #pragma unroll
-        for (int d = 0; d < kMaxDegree; d++) {
-            const float y = odf[nbr[v * kMaxDegree + d]];
-            larger |= x < y;
-            smaller |= y < x;
+            for (int q = 0; q < 4; q++) {
+                const float y0 = odf[w4[q] & 0xffffu], y1 = odf[w4[q] >> 16];
+                larger |= (x < y0) | (x < y1);
+                smaller |= (y0 < x) | (y1 < x);
+            }
+            mx = !larger && smaller;
         }
-        ind[v] = larger ? -1 : (smaller ? 1 : 0);
+        const unsigned msk = __ballot_sync(FULL, mx);
+        if (mx) ind[nm + __popc(msk & lmask)] = v;
+        nm += __popc(msk);
     }
     __syncwarp();
-    return peak_select(P, odf, ind, nr, odf_min, partner_sh, lane);
+    // RELATIVE_PEAK_THRESH * max over maxima of (odf + (-odf_min)), then filter
+    float mm = -FLT_MAX;
+    const float neg_min = -odf_min;
+    for (int c = lane; c < nm; c += kWarp) mm = fmax_ref(mm, odf[ind[c]] + neg_min);
+    mm = warp_max_ref(mm);
+    const float comp_thres = (float)(P.relative_peak_thresh * (double)mm);
+    int n = 0;
+    for (int c0 = 0; c0 < nm; c0 += kWarp) {
+        int v = 0;
+        bool keep = false;
+        if (c0 + lane < nm) {
+            v = ind[c0 + lane];
+            keep = (odf[v] - odf_min) >= comp_thres;
+        }
+        const unsigned msk = __ballot_sync(FULL, keep);
+        __syncwarp();
+        if (keep) ind[n + __popc(msk & lmask)] = v;
+        n += __popc(msk);
+    }
+    __syncwarp();
+    if (n == 0) return 0;
+    if (n < kWarp) {
+        float k = -FLT_MAX;
+        int v = 0;
+        if (lane < n) {
+            v = ind[lane];
+            k = odf[v];
+        }
+        warp_sort_desc(partner_sh, lane, k, v);
+        // greedy minimum-separation filter: candidate i is kept unless a
+        // kept peak before it lies within the separation angle
+        const float3 pv = vert3(P.verts, lane < n ? v : 0);
+        unsigned kept = 1u;
+        for (int i = 1; i < n; i++) {
+            const float3 abc = make_float3(__shfl_sync(FULL, pv.x, i), __shfl_sync(FULL, pv.y, i),
+                                           __shfl_sync(FULL, pv.z, i));
+            float cs = abc.x * pv.x + abc.y * pv.y + abc.z * pv.z;
+            if (P.sphere_symm) cs = fabsf(cs);
+            const bool hit = ((kept >> lane) & 1u) && cs > P.cos_min_sep;
+            if (__ballot_sync(FULL, hit) == 0u) kept |= 1u << i;
+        }
+        __syncwarp();
+        if ((kept >> lane) & 1u) ind[__popc(kept & lmask)] = v;
+        __syncwarp();
+        return __popc(kept);
+    }
+    // 32 or more peaks: the reference skips the sort; serial filter on lane 0
+    if (lane == 0) {
+        int k = 1;
+        for (int i = 1; i < n; i++) {
+            const int vi = ind[i];
+            const float3 abc = vert3(P.verts, vi);
+            int j = 0;
+            for (; j < k; j++) {
+                const float3 d = vert3(P.verts, ind[j]);
+                float cs = abc.x * d.x + abc.y * d.y + abc.z * d.z;
+                if (P.sphere_symm) cs = fabsf(cs);
+                if (cs > P.cos_min_sep) break;
+            }
+            if (j == k) ind[k++] = vi;
+        }
+        n = k;
+    }
+    n = __shfl_sync(FULL, n, 0);
+    __syncwarp();
+    return n;
 }
+
+__device__ __forceinline__ void cp_async16(void *dst, const void *src) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(dst)), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait1() { asm volatile("cp.async.wait_group 1;" ::: "memory"); }
 
 // One CTA = 128 slots, 16 warps.  Warp w owns TMEM lane quadrant w % 4 for
 // the epilogues (the four warps of a quadrant split the columns) and slots
@@ -316,40 +443,64 @@ __global__ void __launch_bounds__(kBThreads, 1)
             }
         }
 
-        // ---- gather: warp w interpolates slots 8w..8w+7 into A1 rows; lane l
-        //      builds k = 8l .. 8l+7 of the non-b0 signal, lanes past the
-        //      non-b0 groups add up the clamped b0 values
-        for (int i = 0; i < kSlots / kBWarps; i++) {
-            const int slot = w * (kSlots / kBWarps) + i;
-            const float4 p4 = s_pt[slot];
-            Corners c;
-            bool inb = false;
-            if (s_live[slot]) inb = trilinear_setup(P, make_float3(p4.x, p4.y, p4.z), c);
-            const int ng = g.HP / 8;
-            float bsum = 0.0f;
-            if (lane < ng) {
-                float x[8];
+        // ---- gather: warp w interpolates slots 8w..8w+7 into A1 rows from the
+        //      volume copy whose T axis holds the hr non-b0 volumes first and
+        //      the b0s after them (padded to TP = 4k): lane l owns float4 l and
+        //      l + 32 of the row; values past hr add up as clamped b0s
+        {
+            DevParams Pg = P;
+            Pg.dimt = g.TP;
+            const int nq = g.TP / 4, nw = nq > g.HP / 4 ? nq : g.HP / 4;
+            for (int i = 0; i < kSlots / kBWarps; i++) {
+                const int slot = w * (kSlots / kBWarps) + i;
+                const float4 p4 = s_pt[slot];
+                Corners c;
+                bool inb = false;
+                if (s_live[slot]) inb = trilinear_setup(Pg, make_float3(p4.x, p4.y, p4.z), c);
+                float bsum = 0.0f;
 #pragma unroll
-                for (int e = 0; e < 8; e++) {
-                    const int k = lane * 8 + e;
-                    x[e] = (inb && k < g.hr) ? trilinear_elem(P.dataf, c, __ldg(A.volidx + k)) : 0.0f;
-                }
-                uint4 hi, lo;
-                split8(x, hi, lo);
-                const uint32_t off = kmajor_off(slot, lane * 8, kSlots);
-                *reinterpret_cast<uint4 *>(R0 + off) = hi;
-                *reinterpret_cast<uint4 *>(R0 + a1_term + off) = lo;
-            } else if (inb) {
-                for (int b = lane - ng; b < g.nb0; b += kWarp - ng) {
-                    const float v = trilinear_elem(P.dataf, c, __ldg(A.volidx + g.hr + b));
-                    bsum += (P.min_signal > v) ? P.min_signal : v;
-                }
-            }
+                for (int r = 0; r < 2; r++) {
+                    const int f = lane + 32 * r;
+                    if (f >= nw) continue;
+                    float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
+                    if (inb && f < nq) {
 #pragma unroll
-            for (int o = 16; o; o >>= 1) bsum += __shfl_xor_sync(FULL, bsum, o);
-            if (lane == 0) {
-                s_pt[slot].w = bsum / (float)g.nb0;
-                s_live[slot] = inb ? 1 : 0;  // outside the data: every attempt would fail
+                        for (int q = 0; q < 8; q++) {
+                            const float4 d = __ldg(reinterpret_cast<const float4 *>(A.dwi + c.base[q]) + f);
+                            acc.x += c.w[q] * d.x;
+                            acc.y += c.w[q] * d.y;
+                            acc.z += c.w[q] * d.z;
+                            acc.w += c.w[q] * d.w;
+                        }
+                    }
+                    float x[4] = {acc.x, acc.y, acc.z, acc.w};
+#pragma unroll
+                    for (int e = 0; e < 4; e++) {
+                        const int k = 4 * f + e;
+                        if (k >= g.hr) {
+                            if (inb && k < g.hr + g.nb0) bsum += (P.min_signal > x[e]) ? P.min_signal : x[e];
+                            x[e] = 0.0f;
+                        }
+                    }
+                    if (4 * f < g.HP) {
+                        const __nv_bfloat162 h01 = __floats2bfloat162_rn(x[0], x[1]);
+                        const __nv_bfloat162 h23 = __floats2bfloat162_rn(x[2], x[3]);
+                        const float2 f01 = __bfloat1622float2(h01), f23 = __bfloat1622float2(h23);
+                        const uint2 hi = make_uint2(*reinterpret_cast<const uint32_t *>(&h01),
+                                                    *reinterpret_cast<const uint32_t *>(&h23));
+                        const uint2 lo = make_uint2(pack_bf16x2(x[0] - f01.x, x[1] - f01.y),
+                                                    pack_bf16x2(x[2] - f23.x, x[3] - f23.y));
+                        const uint32_t off = kmajor_off(slot, 4 * f, kSlots);
+                        *reinterpret_cast<uint2 *>(R0 + off) = hi;
+                        *reinterpret_cast<uint2 *>(R0 + a1_term + off) = lo;
+                    }
+                }
+#pragma unroll
+                for (int o = 16; o; o >>= 1) bsum += __shfl_xor_sync(FULL, bsum, o);
+                if (lane == 0) {
+                    s_pt[slot].w = bsum / (float)g.nb0;
+                    s_live[slot] = inb ? 1 : 0;  // outside the data: every attempt would fail
+                }
             }
         }
         fence_async_smem();
@@ -540,26 +691,36 @@ __global__ void __launch_bounds__(kBThreads, 1)
             __syncthreads();
         }
 
-        // ---- peaks and closest peak: warp w searches slots 8w..8w+7
+        // ---- peaks and closest peak: warp w searches slots 8w..8w+7; the
+        //      next live slot's ODF row is copied in while this one is searched
         {
-            float *odf_sh = reinterpret_cast<float *>(R0) + (size_t)w * 2 * g.vstride;
-            int *ind_sh = reinterpret_cast<int *>(odf_sh + g.vstride);
-            for (int i = 0; i < kSlots / kBWarps; i++) {
-                const int slot = w * (kSlots / kBWarps) + i;
-                if (!s_live[slot]) continue;
+            float *obuf = reinterpret_cast<float *>(R0) + (size_t)w * 3 * g.vstride;
+            int *ind_sh = reinterpret_cast<int *>(obuf + 2 * g.vstride);
+            const int base = w * (kSlots / kBWarps);
+            unsigned live = 0;
+            for (int i = 0; i < kSlots / kBWarps; i++) live |= (s_live[base + i] ? 1u : 0u) << i;
+            const int nch = g.vstride / 4;
+            auto fetch = [&](int slot, float *dst) {
                 const float *src = A.odf + ((size_t)blockIdx.x * kSlots + slot) * g.vstride;
-                float m = -FLT_MAX;
-                for (int v = lane; v < g.V; v += kWarp) {
-                    const float x = __ldcg(src + v);
-                    odf_sh[v] = x;
-                    m = fmax_ref(m, x);
-                }
-                m = warp_max_ref(m);
-                const float thr = (float)(P.pmf_threshold * (double)m);
-                for (int v = lane; v < g.V; v += kWarp)
-                    if (odf_sh[v] < thr) odf_sh[v] = 0;
+                for (int c = lane; c < nch; c += kWarp) cp_async16(dst + 4 * c, src + 4 * c);
+            };
+            int cur = live ? __ffs(live) - 1 : -1;
+            if (cur >= 0) fetch(base + cur, obuf);
+            cp_async_commit();
+            int buf = 0;
+            while (cur >= 0) {
+                const unsigned rest = live & ~((2u << cur) - 1u);
+                const int nxt = rest ? __ffs(rest) - 1 : -1;
+                if (nxt >= 0) fetch(base + nxt, obuf + (buf ^ 1) * g.vstride);
+                cp_async_commit();
+                cp_async_wait1();
                 __syncwarp();
-                const int ndir = peak_directions_nbr(P, odf_sh, ind_sh, g.V, nbr_sh, partner_sh, lane);
+                float *odf_sh = obuf + buf * g.vstride;
+                const int slot = base + cur;
+                float m = -FLT_MAX;
+                for (int v = lane; v < g.V; v += kWarp) m = fmax_ref(m, odf_sh[v]);
+                m = warp_max_ref(m);
+                const int ndir = peaks_sparse(P, odf_sh, ind_sh, g.V, m, nbr_sh, partner_sh, lane);
                 int found = 0;
                 float3 pk = make_float3(0, 0, 0);
                 if (ndir > 0) {
@@ -568,7 +729,10 @@ __global__ void __launch_bounds__(kBThreads, 1)
                 }
                 __syncwarp();
                 if (lane == 0) s_new[slot] = make_float4(pk.x, pk.y, pk.z, found ? 1.0f : 0.0f);
+                cur = nxt;
+                buf ^= 1;
             }
+            asm volatile("cp.async.wait_all;" ::: "memory");
         }
         __syncthreads();
 
@@ -647,6 +811,12 @@ cudaError_t launch_boot_batch_pack(const DevParams &P, const BootBatchGeom &g, v
     boot_batch_pack_kernel<<<256, 256, 0, st>>>(P, g, reinterpret_cast<__nv_bfloat16 *>(B1g),
                                                  reinterpret_cast<__nv_bfloat16 *>(B2g),
                                                  reinterpret_cast<__nv_bfloat16 *>(B3g));
+    return cudaGetLastError();
+}
+
+cudaError_t launch_boot_batch_dwi(const float *src, const int *volidx, long long nvox, int T, int TP,
+                                  float *dst, cudaStream_t st) {
+    boot_batch_dwi_kernel<<<1024, 256, 0, st>>>(src, volidx, nvox, T, TP, dst);
     return cudaGetLastError();
 }
 

@@ -84,7 +84,7 @@ struct csl_tracker {
     DevBuf<short> bb_nbr;
     DevBuf<short> bb_sl_vert;
     DevBuf<long long> bb_half_off;
-    DevBuf<float> bb_odf, bb_pts;
+    DevBuf<float> bb_odf, bb_pts, bb_dwi;
     long long *host_stage = nullptr;  // pinned 16-byte staging for the two totals
     long long last_n = -1, nsl = 0, npts = 0;
     int ok_batch = 0;
@@ -243,6 +243,7 @@ static void release_all(csl_tracker *t) {
     t->bb_half_off.release();
     t->bb_odf.release();
     t->bb_pts.release();
+    t->bb_dwi.release();
     for (auto &e : t->ev)
         if (e) cudaEventDestroy(e);
     if (t->host_stage) cudaFreeHost(t->host_stage);
@@ -440,6 +441,9 @@ int csl_create(const csl_params *params, const csl_inputs *inputs, int device, c
                 if (g.smem > 227 * 1024)
                     return fail(t, CSL_E_INVALID, "boot_fit=1 needs %d B of shared memory per block", g.smem);
                 if ((r = upload(t, t->bb_volidx, volidx.data(), volidx.size()))) return r;
+                CK(t->bb_dwi.ensure(nvox * (size_t)g.TP));
+                CK(launch_boot_batch_dwi(t->dataf.p, t->bb_volidx.p, (long long)nvox, p.dimt, g.TP,
+                                         t->bb_dwi.p, t->own_stream));
                 nbr.resize((size_t)g.nbr_shorts, 0);
                 if ((r = upload(t, t->bb_nbr, nbr.data(), nbr.size()))) return r;
                 CK(t->bb_B1.ensure((size_t)g.nchunk1 * g.b1_chunk));
@@ -546,6 +550,7 @@ static int run_boot_batch(csl_tracker *t, const float *seeds_dev, int ni, int ns
         A.B3g = t->bb_B3.p;
         A.volidx = t->bb_volidx.p;
         A.nbr = t->bb_nbr.p;
+        A.dwi = t->bb_dwi.p;
         A.seeds = seeds_dev;
         A.sl_seed = t->bb_sl_seed.p;
         A.sl_vert = t->bb_sl_vert.p;

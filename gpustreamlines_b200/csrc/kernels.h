@@ -45,6 +45,7 @@ struct BootBatchGeom {
     int HP, N1;         // hr padded to 32; rows of [R ; H] = 2 HP
     int C, N2;          // SH coefficients, padded to 16
     int V, nchunk1, nchunk3, vstride;
+    int TP;             // DWI volumes per voxel in the reordered copy (padded to 4)
     int b1_chunk, b2_bytes, b3_chunk;  // bytes of one packed operand chunk (hi + lo)
     int r0, r1, r2, smem;              // shared-memory regions and total
     int nbr_shorts;                    // V * kMaxDegree, padded to 16 bytes
@@ -56,6 +57,7 @@ struct BootBatchArgs {
     const unsigned char *B3g;  // [nchunk3][2][256 x N2] packed sampling matrix
     const int *volidx;         // [T] volume indices: the hr non-b0 volumes, then the b0s
     const short *nbr;          // [V][kMaxDegree] sphere neighbours, padded with the vertex itself
+    const float *dwi;          // [X,Y,Z,TP] DWI with the T axis in volidx order
     const float *seeds;
     const int *sl_seed;        // streamline -> seed (batch-local)
     const short *sl_vert;      // streamline -> initial vertex
@@ -75,6 +77,8 @@ struct BootBatchArgs {
 BootBatchGeom boot_batch_geom(const DevParams &P, int hr, int nb0);
 cudaError_t launch_boot_batch_pack(const DevParams &P, const BootBatchGeom &g, void *B1g, void *B2g,
                                    void *B3g, cudaStream_t st);
+cudaError_t launch_boot_batch_dwi(const float *src, const int *volidx, long long nvox, int T, int TP,
+                                  float *dst, cudaStream_t st);
 cudaError_t launch_boot_batch_prep(const int *npeaks, const int *sl_off, const short *peaks, int max_store,
                                    int n, int *sl_seed, short *sl_vert, int *status, cudaStream_t st);
 cudaError_t launch_boot_batch_join(const int *half_len, const int *sl_seed, int nsl, int *out_len,
