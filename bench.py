@@ -368,7 +368,23 @@ def main():
     if model == "PROB":
         roofline["traffic_source"] = "ncu dram__bytes_read+write per step at 20k seeds x steps"
     if gcfg.get("fit") == "bf16x3":
-        roofline["kernel"] = "boot_batch_kernel (pass 2, tcgen05 BF16x3)"
+        # tensor roofline of the batched fit: algorithmic FP32-equivalent FLOP per
+        # attempt (each step takes >= 1 attempt) against the measured BF16 peak;
+        # the BF16x3 split issues 3x these on the tensor pipe
+        nc = dg.delta_nr
+        hr = int((dg.b0s_mask == 0).sum())
+        flop = 2 * 2 * hr * hr + 2 * nc * hr + 2 * nc * dg.sampling_matrix.shape[0]
+        tpeak = None
+        path = os.path.join(HERE, "MEASURED_PEAKS.json")
+        if os.path.exists(path):
+            with open(path) as f:
+                tpeak = float(json.load(f).get("bf16_tflops", 0) or 0) or None
+        tach = steps_per_batch * flop / (p2 / 1e3) / 1e12
+        roofline = {"bound": "tensor", "achieved": tach, "peak": tpeak or 1590.0, "unit": "TFLOP/s",
+                    "frac": tach / (tpeak or 1590.0), "traffic": None,
+                    "kernel": "boot_batch_kernel (pass 2, tcgen05 BF16x3)",
+                    "peak_source": "measured MEASURED_PEAKS bf16_tflops" if tpeak else "fallback",
+                    "algorithmic_flop_per_step": flop, "issued_bf16_flop_per_step": 3 * flop}
     extra = {}
     if model == "PTT":
         frac = int(np.round(0.5 / dg.target_short_step))  # propagation sub-steps per point

@@ -64,7 +64,7 @@ EXPORTS = (
     "csl_create", "csl_destroy", "csl_propagate", "csl_propagate_device", "csl_counts",
     "csl_fetch", "csl_device_results", "csl_seed_peaks", "csl_get_direction",
     "csl_device_constants", "csl_philox_stream", "csl_last_error", "csl_version",
-    "csl_batch_timings", "csl_track_noalloc",
+    "csl_batch_timings", "csl_track_noalloc", "csl_boot_odf",
 )
 
 
@@ -94,6 +94,7 @@ def load(path: str | None = None):
     lib.csl_device_constants.argtypes = [vp, _fp, _fp]
     lib.csl_batch_timings.argtypes = [vp, _fp, _ip]
     lib.csl_track_noalloc.argtypes = [vp, vp, ll, ll, C.c_int, vp, vp, vp, vp]
+    lib.csl_boot_odf.argtypes = [vp, vp, vp, ll, C.c_int, vp, C.c_int, vp]
     lib.csl_philox_stream.argtypes = [C.c_ulonglong, C.c_ulonglong, C.c_ulonglong, ll,
                                       C.POINTER(C.c_uint)]
     lib.csl_last_error.argtypes = [vp, C.c_char_p, C.c_int]
@@ -239,6 +240,13 @@ class Handle:
                                              int(rng_index_base), int(max_peaks),
                                              C.c_void_p(counts_ptr), C.c_void_p(lens_ptr),
                                              C.c_void_p(points_ptr), stream))
+
+    def boot_odf(self, points_ptr: int, resample_ptr: int, n: int, fit: int, odf_ptr: int, odf_stride: int,
+                 stream: int | None = None):
+        """ODF of one bootstrap fit per point with given resample indices, into
+        a device buffer (fit 0: per-warp FP32, 1: batched BF16x3; see the C header)."""
+        self._chk(self.lib.csl_boot_odf(self.h, C.c_void_p(points_ptr), C.c_void_p(resample_ptr), int(n),
+                                        int(fit), C.c_void_p(odf_ptr), int(odf_stride), stream))
 
     def timings(self):
         """(pass1_ms, gap_ms, pass2_ms, compact_ms), pass-2 runs of the last batch."""

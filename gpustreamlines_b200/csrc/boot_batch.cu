@@ -408,7 +408,16 @@ __global__ void __launch_bounds__(kBThreads, 1)
     for (;;) {
         // ---- refill empty slots from the queue of streamline halves
         if (t < kSlots) {
-            if (my_h < 0 && !queue_empty) {
+            if (my_h < 0 && !queue_empty && A.nprobe > 0) {
+                const int h = atomicAdd(A.hq, 1);
+                if (h >= A.nprobe) {
+                    queue_empty = true;
+                } else {
+                    my_h = h;
+                    my_pt = make_float3(A.probe_pts[3 * h], A.probe_pts[3 * h + 1], A.probe_pts[3 * h + 2]);
+                    my_i = 1;
+                }
+            } else if (my_h < 0 && !queue_empty) {
                 const int h = atomicAdd(A.hq, 1);
                 if (h >= 2 * A.nsl) {
                     queue_empty = true;
@@ -563,7 +572,8 @@ __global__ void __launch_bounds__(kBThreads, 1)
             const int h = s_h[eslot];
             const bool live = s_live[eslot] != 0;
             const float denom = s_pt[eslot].w;
-            if (live && h != rng_h) {
+            const int *pidx = A.nprobe > 0 ? A.probe_idx + (size_t)(h >= 0 ? h : 0) * g.hr : nullptr;
+            if (live && !pidx && h != rng_h) {
                 const int sl = h >> 1, half = h & 1;
                 rng.init(P.rng_seed,
                          kBatchSubseqBase + 8ull * (unsigned long long)(sl + A.rng_base) + 4 * half + part, 0);
@@ -580,7 +590,7 @@ __global__ void __launch_bounds__(kBThreads, 1)
                         const int j = 16 * b + gq * 8 + e;
                         y[e] = 0.0f;
                         if (live && j < g.hr) {
-                            const int src = (int)(rng.next() % (unsigned)g.hr);
+                            const int src = pidx ? pidx[j] : (int)(rng.next() % (unsigned)g.hr);
                             float x = hv[gq * 8 + e] + rb[src];
                             x = (P.min_signal > x) ? P.min_signal : x;
                             x = x / denom;
@@ -646,6 +656,7 @@ __global__ void __launch_bounds__(kBThreads, 1)
 
         // ---- MMA 3 in 256-vertex chunks: ODF rows -> L2 scratch
         float *e_odf = A.odf + ((size_t)blockIdx.x * kSlots + eslot) * g.vstride;
+        if (A.nprobe > 0 && s_live[eslot]) e_odf = A.probe_odf + (size_t)s_h[eslot] * A.probe_stride;
         for (int ch = 0; ch < g.nchunk3; ch++) {
             if (t == 0 && ok) {
                 mbar_arrive_expect_tx(&bars[5], (uint32_t)g.b3_chunk);
@@ -689,6 +700,11 @@ __global__ void __launch_bounds__(kBThreads, 1)
             }
             tc_fence_before();
             __syncthreads();
+        }
+
+        if (A.nprobe > 0) {  // probe mode: the ODF rows are the output
+            if (t < kSlots) my_h = -1;
+            continue;
         }
 
         // ---- peaks and closest peak: warp w searches slots 8w..8w+7; the

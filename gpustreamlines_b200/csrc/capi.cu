@@ -740,6 +740,53 @@ static int run_batch(csl_tracker *t, const float *seeds_dev, long long n, long l
     return CSL_OK;
 }
 
+int csl_boot_odf(csl_tracker *t, const float *points_dev, const int *resample_dev, long long n, int fit,
+                 float *odf_dev, int odf_stride, void *stream) {
+    if (!t) return fail(nullptr, CSL_E_INVALID, "NULL tracker");
+    const DevParams &P = t->P;
+    if (P.model != CSA && P.model != OPDT) return fail(t, CSL_E_STATE, "csl_boot_odf needs a bootstrap tracker");
+    if (n < 0 || n > (1ll << 30)) return fail(t, CSL_E_INVALID, "bad point count");
+    if (fit != 0 && fit != 1) return fail(t, CSL_E_INVALID, "fit must be 0 or 1");
+    if (fit == 1 && t->hp.boot_fit != 1)
+        return fail(t, CSL_E_STATE, "fit=1 needs a tracker created with boot_fit=1");
+    if (odf_stride < P.samplm_nr || odf_stride % 4 != 0)
+        return fail(t, CSL_E_INVALID, "odf_stride must be >= samplm_nr and a multiple of 4");
+    if (n == 0) return CSL_OK;
+    if (!points_dev || !resample_dev || !odf_dev) return fail(t, CSL_E_INVALID, "NULL buffer");
+    CK(cudaSetDevice(t->device));
+    cudaStream_t st = stream ? (cudaStream_t)stream : t->own_stream;
+    CK(cudaMemsetAsync(odf_dev, 0, (size_t)n * odf_stride * sizeof(float), st));
+    if (fit == 0) {
+        CK(launch_boot_odf_plain(P, points_dev, resample_dev, (int)n, odf_dev, odf_stride, st));
+    } else {
+        const BootBatchGeom &g = t->bgeom;
+        BootBatchArgs A{};
+        A.B1g = t->bb_B1.p;
+        A.B2g = t->bb_B2.p;
+        A.B3g = t->bb_B3.p;
+        A.volidx = t->bb_volidx.p;
+        A.nbr = t->bb_nbr.p;
+        A.dwi = t->bb_dwi.p;
+        A.hq = t->bb_hq.p;
+        A.odf = t->bb_odf.p;
+        A.pts = t->bb_pts.p;
+        A.status = t->status.p;
+        A.nprobe = (int)n;
+        A.probe_pts = points_dev;
+        A.probe_idx = resample_dev;
+        A.probe_odf = odf_dev;
+        A.probe_stride = odf_stride;
+        CK(cudaMemsetAsync(t->bb_hq.p, 0, sizeof(int), st));
+        CK(cudaMemsetAsync(t->status.p, 0, sizeof(int), st));
+        CK(launch_boot_batch(P, g, A, t->partner.p, t->nsm, st));
+        CK(cudaMemcpyAsync(t->host_stage, t->status.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+    }
+    CK(cudaStreamSynchronize(st));
+    if (fit == 1 && ((int)(t->host_stage[0] & 0xffffffff) & ST_WAIT_TIMEOUT))
+        return fail(t, CSL_E_KERNEL, "tensor-core pipeline wait timed out");
+    return CSL_OK;
+}
+
 int csl_propagate_device(csl_tracker *t, const float *seeds_dev, long long n, long long rng_index_base,
                          void *stream) {
     if (!t) return fail(nullptr, CSL_E_INVALID, "NULL tracker");

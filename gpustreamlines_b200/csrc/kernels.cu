@@ -322,6 +322,65 @@ __global__ void get_direction_kernel(DevParams P, const int *partner, const floa
     }
 }
 
+// ODF of one bootstrap fit at given points with given resample indices, in
+// the per-warp FP32 arithmetic of the tracking path (boot_get_direction up
+// to the sphere sampling; boot.cu:393-560): the plain-fit side of the
+// accuracy measurement.  One warp per point; rows of length vstride.
+template <int MODEL>
+__global__ void boot_odf_plain_kernel(DevParams P, const float *pts, const int *idx, int n, float *odf,
+                                      int vstride) {
+    extern __shared__ float smem[];
+    const int warp = threadIdx.x / kWarp, lane = threadIdx.x & 31;
+    const WarpBufs W = carve(P, smem + kMaxSortLayers * kWarp, warp, false, nullptr);
+    const int q = blockIdx.x * (blockDim.x / kWarp) + warp;
+    if (q >= n) return;
+    const int T = P.dimt, hr = P.hr_side, nr = P.samplm_nr;
+    const float3 point = make_float3(pts[3 * q], pts[3 * q + 1], pts[3 * q + 2]);
+    Corners c;
+    const bool inb = trilinear_setup(P, point, c);
+    float *out = odf + (size_t)q * vstride;
+    if (!inb) {
+        for (int j = lane; j < nr; j += kWarp) out[j] = 0.0f;
+        return;
+    }
+    for (int t = lane; t < T; t += kWarp) W.vox[t] = trilinear_elem(P.dataf, c, t);
+    __syncwarp();
+    mask_get(T, P.b0s_mask, W.vox, W.msk, lane);
+    __syncwarp();
+    ndotp_rows<0>(hr, hr, W.msk, P.R, W.r, lane);
+    ndotp_rows<0>(hr, hr, W.msk, P.H, W.h, lane);
+    __syncwarp();
+    for (int j = lane; j < hr; j += kWarp) W.h[j] += W.r[idx[(size_t)q * hr + j]];
+    __syncwarp();
+    mask_put(T, P.b0s_mask, W.h, W.vox, lane);
+    __syncwarp();
+    for (int j = lane; j < T; j += kWarp) {
+        const float x = W.vox[j];
+        W.vox[j] = (P.min_signal > x) ? P.min_signal : x;
+    }
+    __syncwarp();
+    const float denom = avg_mask(T, P.b0s_mask, W.vox, lane);
+    for (int j = lane; j < T; j += kWarp) W.vox[j] /= denom;
+    __syncwarp();
+    mask_get(T, P.b0s_mask, W.vox, W.msk, lane);
+    __syncwarp();
+    if (MODEL == OPDT) {
+        ndotp_rows<1>(P.delta_nr, hr, W.msk, P.delta_q, W.r, lane);
+        ndotp_rows<0>(P.delta_nr, hr, W.msk, P.delta_b, W.h, lane);
+        __syncwarp();
+        for (int j = lane; j < P.delta_nr; j += kWarp) W.r[j] -= W.h[j];
+        __syncwarp();
+    } else {
+        ndotp_rows<2>(P.delta_nr, hr, W.msk, P.delta_q, W.r, lane);
+        __syncwarp();
+        if (lane == 0) W.r[0] = kN0Const;
+        __syncwarp();
+    }
+    ndotp_rows<0>(nr, P.delta_nr, W.r, P.sampling, W.h, lane);
+    __syncwarp();
+    for (int j = lane; j < nr; j += kWarp) out[j] = W.h[j];
+}
+
 // ---------------------------------------------------------------------------
 // launchers
 
@@ -462,4 +521,25 @@ cudaError_t exclusive_scan_i64(void *tmp, size_t tmp_bytes, const int *in, long 
     return e != cudaSuccess ? e : cudaGetLastError();
 }
 
+}  // namespace csl
+
+namespace csl {
+cudaError_t launch_boot_odf_plain(const DevParams &P, const float *pts, const int *idx, int n, float *odf,
+                                  int vstride, cudaStream_t st) {
+    if (n <= 0) return cudaSuccess;
+    const int block = 128;
+    const int smem = smem_bytes(P, block / kWarp, false);
+    const int grid = (n + 3) / 4;
+    cudaError_t e;
+    if (P.model == OPDT) {
+        e = set_smem(boot_odf_plain_kernel<OPDT>, smem);
+        if (e != cudaSuccess) return e;
+        boot_odf_plain_kernel<OPDT><<<grid, block, smem, st>>>(P, pts, idx, n, odf, vstride);
+    } else {
+        e = set_smem(boot_odf_plain_kernel<CSA>, smem);
+        if (e != cudaSuccess) return e;
+        boot_odf_plain_kernel<CSA><<<grid, block, smem, st>>>(P, pts, idx, n, odf, vstride);
+    }
+    return cudaGetLastError();
+}
 }  // namespace csl

@@ -69,6 +69,14 @@ struct BootBatchArgs {
     unsigned long long *pool_count;
     float *pool;
     unsigned long long pool_cap;
+    // probe mode (nprobe > 0): work items are points, not streamline halves;
+    // each gets one fit with the given resample indices and its ODF row is
+    // written to probe_odf[item * probe_stride]; no tracking
+    int nprobe;
+    const float *probe_pts;    // [nprobe,3]
+    const int *probe_idx;      // [nprobe][hr] bootstrap source index of each non-b0 volume
+    float *probe_odf;          // [nprobe][probe_stride]
+    int probe_stride;
     int *half_len;             // [2 nsl] points per half (seed included)
     long long *half_off;       // [2 nsl] pool offset of each half (-1 when the pool overflowed)
     int *status;
@@ -86,6 +94,8 @@ cudaError_t launch_boot_batch_join(const int *half_len, const int *sl_seed, int 
 cudaError_t launch_gather_halves(const float *pool, const long long *half_off, const int *half_len,
                                  const long long *pt_off, int nsl, float *out, int grid, cudaStream_t st);
 cudaError_t boot_batch_set_smem(const BootBatchGeom &g);
+cudaError_t launch_boot_odf_plain(const DevParams &P, const float *pts, const int *idx, int n, float *odf,
+                                  int vstride, cudaStream_t st);
 cudaError_t launch_boot_batch(const DevParams &P, const BootBatchGeom &g, const BootBatchArgs &A,
                               const int *partner, int grid, cudaStream_t st);
 

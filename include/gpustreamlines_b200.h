@@ -217,6 +217,19 @@ int csl_track_noalloc(csl_tracker *t, const float *seeds_dev, long long n, long 
 int csl_last_error(const csl_tracker *t, char *buf, int buflen);
 
 /* Library version string. */
+/*
+ * Measurement entry point (no counterpart in the reference): the ODF of one
+ * bootstrap fit at each of n device points, with the bootstrap source index
+ * of every non-b0 volume given (resample[n][hr], 0 <= index < hr) instead of
+ * drawn, so that fits can be compared at a fixed state.  fit = 0: the
+ * per-warp FP32 arithmetic of the tracking path; fit = 1: the batched
+ * tensor-core BF16x3 fit (needs a tracker created with boot_fit = 1).  Row i
+ * of odf (stride odf_stride >= samplm_nr, a multiple of 4) receives the
+ * samplm_nr ODF values; points outside the data give a zero row.
+ */
+int csl_boot_odf(csl_tracker *tracker, const float *points_dev, const int *resample_dev, long long n, int fit,
+                 float *odf_dev, int odf_stride, void *stream);
+
 const char *csl_version(void);
 
 #ifdef __cplusplus
