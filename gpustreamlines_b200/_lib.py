@@ -64,7 +64,7 @@ EXPORTS = (
     "csl_create", "csl_destroy", "csl_propagate", "csl_propagate_device", "csl_counts",
     "csl_fetch", "csl_device_results", "csl_seed_peaks", "csl_get_direction",
     "csl_device_constants", "csl_philox_stream", "csl_last_error", "csl_version",
-    "csl_batch_timings", "csl_track_noalloc", "csl_boot_odf",
+    "csl_batch_timings", "csl_track_noalloc", "csl_boot_odf", "csl_odf_volume",
 )
 
 
@@ -95,6 +95,7 @@ def load(path: str | None = None):
     lib.csl_batch_timings.argtypes = [vp, _fp, _ip]
     lib.csl_track_noalloc.argtypes = [vp, vp, ll, ll, C.c_int, vp, vp, vp, vp]
     lib.csl_boot_odf.argtypes = [vp, vp, vp, ll, C.c_int, vp, C.c_int, vp]
+    lib.csl_odf_volume.argtypes = [vp, ll, C.c_int, vp, C.c_int, C.c_int, vp, vp, ll, _fp, vp]
     lib.csl_philox_stream.argtypes = [C.c_ulonglong, C.c_ulonglong, C.c_ulonglong, ll,
                                       C.POINTER(C.c_uint)]
     lib.csl_last_error.argtypes = [vp, C.c_char_p, C.c_int]

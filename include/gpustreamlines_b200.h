@@ -230,6 +230,20 @@ int csl_last_error(const csl_tracker *t, char *buf, int buflen);
 int csl_boot_odf(csl_tracker *tracker, const float *points_dev, const int *resample_dev, long long n, int fit,
                  float *odf_dev, int odf_stride, void *stream);
 
+/*
+ * ODF / PMF volume from SH coefficients on the tensor cores (the host step
+ * before tracking in run_gpu_streamlines.py:357-380, fit.odf(sphere) clipped
+ * to >= 0 for the probabilistic getter):
+ *     out[x, v] = sum_c coef[x, c] * basis[v, c], clipped at 0 when clip != 0
+ * coef [nvox, ncoef] f32 (ncoef <= 64), basis [nvert, ncoef] f32 (nvert <=
+ * 1024), out [nvox, nvert] f32, all device memory; products in BF16x3 with
+ * FP32 accumulation (~1e-5 of the row scale).  workspace: caller-owned device
+ * memory of at least ceil(nvert / 256) * 256 * ceil16(ncoef) * 4 + 16 bytes.
+ * *ms_out (optional) receives the kernel time.  Returns CSL_OK or CSL_E_*.
+ */
+int csl_odf_volume(const float *coef_dev, long long nvox, int ncoef, const float *basis_dev, int nvert, int clip,
+                   float *out_dev, void *workspace_dev, long long workspace_bytes, float *ms_out, void *stream);
+
 const char *csl_version(void);
 
 #ifdef __cplusplus
