@@ -65,6 +65,7 @@ EXPORTS = (
     "csl_fetch", "csl_device_results", "csl_seed_peaks", "csl_get_direction",
     "csl_device_constants", "csl_philox_stream", "csl_last_error", "csl_version",
     "csl_batch_timings", "csl_track_noalloc", "csl_boot_odf", "csl_odf_volume",
+    "csl_compress", "csl_fetch_compressed",
 )
 
 
@@ -95,6 +96,9 @@ def load(path: str | None = None):
     lib.csl_batch_timings.argtypes = [vp, _fp, _ip]
     lib.csl_track_noalloc.argtypes = [vp, vp, ll, ll, C.c_int, vp, vp, vp, vp]
     lib.csl_boot_odf.argtypes = [vp, vp, vp, ll, C.c_int, vp, C.c_int, vp]
+    lib.csl_compress.argtypes = [vp, C.POINTER(C.c_double), C.c_double, C.c_double, C.c_int, C.c_int,
+                                 C.POINTER(ll)]
+    lib.csl_fetch_compressed.argtypes = [vp, _ip, _fp]
     lib.csl_odf_volume.argtypes = [vp, ll, C.c_int, vp, C.c_int, C.c_int, vp, vp, ll, _fp, vp]
     lib.csl_philox_stream.argtypes = [C.c_ulonglong, C.c_ulonglong, C.c_ulonglong, ll,
                                       C.POINTER(C.c_uint)]
@@ -248,6 +252,23 @@ class Handle:
         a device buffer (fit 0: per-warp FP32, 1: batched BF16x3; see the C header)."""
         self._chk(self.lib.csl_boot_odf(self.h, C.c_void_p(points_ptr), C.c_void_p(resample_ptr), int(n),
                                         int(fit), C.c_void_p(odf_ptr), int(odf_stride), stream))
+
+    def compress(self, affine=None, tol_error=0.1, max_segment_length=10.0, minlen=0, maxlen=None):
+        """Linearise the last batch on the device in world coordinates; returns
+        (counts per streamline, 0 = dropped; kept points [n, 3] float32)."""
+        aff = None
+        if affine is not None:
+            a = np.ascontiguousarray(np.asarray(affine, dtype=np.float64).reshape(4, 4))
+            aff = a.ctypes.data_as(C.POINTER(C.c_double))
+        mx = 2**31 - 1 if maxlen is None or not np.isfinite(maxlen) else int(min(maxlen, 2**31 - 1))
+        npts = C.c_longlong()
+        self._chk(self.lib.csl_compress(self.h, aff, float(tol_error), float(max_segment_length),
+                                        int(max(0, minlen)), mx, C.byref(npts)))
+        nsl, _ = self.counts()
+        cnt = np.empty(nsl, dtype=np.int32)
+        pts = np.empty((npts.value, 3), dtype=np.float32)
+        self._chk(self.lib.csl_fetch_compressed(self.h, iptr(cnt), fptr(pts)))
+        return cnt, pts
 
     def timings(self):
         """(pass1_ms, gap_ms, pass2_ms, compact_ms), pass-2 runs of the last batch."""

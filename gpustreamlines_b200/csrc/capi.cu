@@ -85,6 +85,12 @@ struct csl_tracker {
     DevBuf<short> bb_sl_vert;
     DevBuf<long long> bb_half_off;
     DevBuf<float> bb_odf, bb_pts, bb_dwi;
+    // compression of the last batch (csl_compress)
+    DevBuf<float> cmp_world, cmp_pts;
+    DevBuf<unsigned char> cmp_keep;
+    DevBuf<int> cmp_cnt;
+    DevBuf<long long> cmp_off;
+    long long cmp_npts = -1;
     long long *host_stage = nullptr;  // pinned 16-byte staging for the two totals
     long long last_n = -1, nsl = 0, npts = 0;
     int ok_batch = 0;
@@ -244,6 +250,11 @@ static void release_all(csl_tracker *t) {
     t->bb_odf.release();
     t->bb_pts.release();
     t->bb_dwi.release();
+    t->cmp_world.release();
+    t->cmp_pts.release();
+    t->cmp_keep.release();
+    t->cmp_cnt.release();
+    t->cmp_off.release();
     for (auto &e : t->ev)
         if (e) cudaEventDestroy(e);
     if (t->host_stage) cudaFreeHost(t->host_stage);
@@ -616,6 +627,7 @@ static int run_batch(csl_tracker *t, const float *seeds_dev, long long n, long l
                      cudaStream_t st) {
     const DevParams &P = t->P;
     t->ok_batch = 0;
+    t->cmp_npts = -1;
     t->nsl = t->npts = 0;
     t->last_n = n;
     t->last_stream = st;
@@ -784,6 +796,54 @@ int csl_boot_odf(csl_tracker *t, const float *points_dev, const int *resample_de
     CK(cudaStreamSynchronize(st));
     if (fit == 1 && ((int)(t->host_stage[0] & 0xffffffff) & ST_WAIT_TIMEOUT))
         return fail(t, CSL_E_KERNEL, "tensor-core pipeline wait timed out");
+    return CSL_OK;
+}
+
+int csl_compress(csl_tracker *t, const double *affine16, double tol_error, double max_segment_length,
+                 int minlen, int maxlen, long long *npts_out) {
+    if (!t) return fail(nullptr, CSL_E_INVALID, "NULL tracker");
+    if (!t->ok_batch) return fail(t, CSL_E_STATE, "no completed batch to compress");
+    if (!(tol_error >= 0.0) || !(max_segment_length > 0.0))
+        return fail(t, CSL_E_INVALID, "tol_error must be >= 0 and max_segment_length > 0");
+    CK(cudaSetDevice(t->device));
+    cudaStream_t st = t->last_stream ? t->last_stream : t->own_stream;
+    const int nsl = (int)t->nsl;
+    const long long npts = t->npts;
+    CK(t->cmp_world.ensure((size_t)std::max<long long>(npts, 1) * 3));
+    CK(t->cmp_pts.ensure((size_t)std::max<long long>(npts, 1) * 3));
+    CK(t->cmp_keep.ensure((size_t)std::max<long long>(npts, 1)));
+    CK(t->cmp_cnt.ensure((size_t)nsl + 1));
+    CK(t->cmp_off.ensure((size_t)nsl + 1));
+    CK(launch_compress(t->points.p, npts, affine16, t->pt_off.p, t->out_len.p, nsl, minlen, maxlen, tol_error,
+                       max_segment_length, t->cmp_world.p, t->cmp_keep.p, t->cmp_cnt.p, st));
+    CK(cudaMemsetAsync(t->cmp_cnt.p + nsl, 0, sizeof(int), st));
+    size_t tmpb = 0;
+    CK(scan_temp_bytes(nsl + 1, &tmpb));
+    if (tmpb > t->scan_tmp.cap) {
+        CK(cudaStreamSynchronize(st));
+        CK(t->scan_tmp.ensure(tmpb));
+    }
+    CK(exclusive_scan_i64(t->scan_tmp.p, t->scan_tmp.cap, t->cmp_cnt.p, t->cmp_off.p, nsl + 1, st));
+    CK(launch_compress_gather(t->cmp_world.p, t->pt_off.p, t->out_len.p, t->cmp_keep.p, t->cmp_off.p, nsl,
+                              t->cmp_pts.p, st));
+    CK(cudaMemcpyAsync(t->host_stage, t->cmp_off.p + nsl, sizeof(long long), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    t->cmp_npts = t->host_stage[0];
+    if (npts_out) *npts_out = t->cmp_npts;
+    return CSL_OK;
+}
+
+int csl_fetch_compressed(csl_tracker *t, int *counts_host, float *points_host) {
+    if (!t) return fail(nullptr, CSL_E_INVALID, "NULL tracker");
+    if (!t->ok_batch || t->cmp_npts < 0) return fail(t, CSL_E_STATE, "call csl_compress first");
+    CK(cudaSetDevice(t->device));
+    cudaStream_t st = t->last_stream ? t->last_stream : t->own_stream;
+    if (counts_host && t->nsl > 0)
+        CK(cudaMemcpyAsync(counts_host, t->cmp_cnt.p, (size_t)t->nsl * sizeof(int), cudaMemcpyDeviceToHost, st));
+    if (points_host && t->cmp_npts > 0)
+        CK(cudaMemcpyAsync(points_host, t->cmp_pts.p, (size_t)t->cmp_npts * 3 * sizeof(float),
+                           cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
     return CSL_OK;
 }
 

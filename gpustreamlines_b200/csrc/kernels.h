@@ -99,6 +99,13 @@ cudaError_t launch_boot_odf_plain(const DevParams &P, const float *pts, const in
 cudaError_t launch_boot_batch(const DevParams &P, const BootBatchGeom &g, const BootBatchArgs &A,
                               const int *partner, int grid, cudaStream_t st);
 
+cudaError_t launch_compress(const float *pts, long long npts, const double *affine16, const long long *off,
+                            const int *len, int nsl, int minlen, int maxlen, double tol, double maxseg, float *world,
+                            unsigned char *keep, int *cnt, cudaStream_t st);
+cudaError_t launch_compress_gather(const float *world, const long long *off, const int *len,
+                                   const unsigned char *keep, const long long *coff, int nsl, float *out,
+                                   cudaStream_t st);
+
 cudaError_t scan_temp_bytes(int n, size_t *bytes);
 // Morton-sort the seeds (perm = position -> seed) and split the order into
 // per-block ranges; with tmp == nullptr only reports the sort's temp size.

@@ -13,7 +13,7 @@ import logging
 
 import numpy as np
 
-from .io import ArraySequence, Space, StatefulTractogram, Tractogram, TrxFile, compress_streamlines
+from .io import ArraySequence, Space, StatefulTractogram, Tractogram, TrxFile
 
 logger = logging.getLogger("GPUStreamlines")
 
@@ -87,16 +87,23 @@ class GenericTracker:
                            init_as=trx_reference)
         trx_reference.close()
         for idx in range(int(nchunks)):
-            self.seed_propagator.propagate(seeds[idx * global_chunk_sz:(idx + 1) * global_chunk_sz])
-            tractogram = Tractogram(self.seed_propagator.as_array_sequence(),
-                                    affine_to_rasmm=trx_file.header["VOXEL_TO_RASMM"])
-            if len(tractogram) == 0:
-                continue
-            tractogram.to_world()
-            sls = tractogram.streamlines
+            chunk = seeds[idx * global_chunk_sz:(idx + 1) * global_chunk_sz]
             if self._linearize():
-                sls = ArraySequence(compress_streamlines(list(sls), tol_error=self._tol_error(),
-                                                         max_segment_length=self._max_segment_length()))
+                # world transform and linearisation on the device; only the
+                # compressed points come back (the reference does both on the host)
+                self.seed_propagator.propagate_compressed(chunk, trx_file.header["VOXEL_TO_RASMM"],
+                                                          self._tol_error(), self._max_segment_length())
+                sls = self.seed_propagator.as_compressed_sequence()
+                if len(sls) == 0:
+                    continue
+            else:
+                self.seed_propagator.propagate(chunk)
+                tractogram = Tractogram(self.seed_propagator.as_array_sequence(),
+                                        affine_to_rasmm=trx_file.header["VOXEL_TO_RASMM"])
+                if len(tractogram) == 0:
+                    continue
+                tractogram.to_world()
+                sls = tractogram.streamlines
             before = trx_file.header["NB_STREAMLINES"]
             trx_file.append_block(np.asarray(sls._data, dtype=self._pos_dtype()), sls._lengths)
             if trx_file.header["NB_STREAMLINES"] != before:

@@ -68,6 +68,44 @@ class SeedBatchPropagator:
         # the reference advances rng_offset per chunk (its kernels ignore it)
         self.gpu_tracker.rng_offset += self.nseeds
 
+    def propagate_compressed(self, seeds, affine, tol_error, max_segment_length):
+        """``propagate`` followed by the world transform and the linearisation
+        on the device (``csl_compress``); only the compressed points are copied
+        to the host.  Results: ``as_compressed_sequence()``."""
+        seeds = np.ascontiguousarray(np.asarray(seeds), dtype=np.float32).reshape(-1, 3)
+        self.nseeds = len(seeds)
+        self.nseeds_per_gpu = (self.nseeds + self.ngpus - 1) // self.ngpus
+        if not self.gpu_tracker._allocated:
+            raise RuntimeError("GPUTracker must be entered (use `with`) before tracking")
+
+        def run(ii):
+            start, cnt = self._shard(ii)
+            h = self.gpu_tracker.handles[ii]
+            h.propagate(seeds[start:start + cnt], rng_index_base=0)
+            counts, pts = h.compress(affine, tol_error, max_segment_length, int(max(0, self.minlen)),
+                                     self.maxlen)
+            return ii, counts[counts > 0], pts
+
+        if self.ngpus == 1:
+            results = [run(0)]
+        else:
+            with ThreadPoolExecutor(self.ngpus) as ex:
+                results = list(ex.map(run, range(self.ngpus)))
+        self.c_lens = [None] * self.ngpus
+        self.c_pts = [None] * self.ngpus
+        for ii, L, P in results:
+            self.c_lens[ii] = L
+            self.c_pts[ii] = P
+        self.gpu_tracker.rng_offset += self.nseeds
+
+    def as_compressed_sequence(self):
+        """Compressed world-space streamlines of the last ``propagate_compressed``."""
+        lens = [x for x in self.c_lens if x is not None and len(x)]
+        pts = [p for x, p in zip(self.c_lens, self.c_pts) if x is not None and len(x)]
+        if not lens:
+            return ArraySequence()
+        return ArraySequence.from_flat(np.concatenate(pts), np.concatenate(lens))
+
     def _keep(self, lens):
         return (lens >= self.minlen) & (lens <= self.maxlen)
 

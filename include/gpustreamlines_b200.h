@@ -244,6 +244,21 @@ int csl_boot_odf(csl_tracker *tracker, const float *points_dev, const int *resam
 int csl_odf_volume(const float *coef_dev, long long nvox, int ncoef, const float *basis_dev, int nvert, int clip,
                    float *out_dev, void *workspace_dev, long long workspace_bytes, float *ms_out, void *stream);
 
+/*
+ * Linearise the last batch's streamlines on the device (replaces the host
+ * Tractogram.to_world() + DIPY compress_streamlines of generic_tracker.py:
+ * 133-144): points are mapped to world coordinates with the 4x4 affine
+ * (row-major doubles; NULL = identity), then compressed with tolerance
+ * tol_error and segments of at most max_segment_length (world units);
+ * streamlines with fewer than minlen or more than maxlen points are dropped
+ * (count 0).  *npts_out receives the number of kept points.
+ */
+int csl_compress(csl_tracker *tracker, const double *affine16, double tol_error, double max_segment_length,
+                 int minlen, int maxlen, long long *npts_out);
+/* Compressed results of csl_compress: counts[n_streamlines] (0 = dropped) and
+ * the kept world points [npts_out, 3], streamlines in order. */
+int csl_fetch_compressed(csl_tracker *tracker, int *counts_host, float *points_host);
+
 const char *csl_version(void);
 
 #ifdef __cplusplus
