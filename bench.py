@@ -53,6 +53,8 @@ def parse():
     ap.add_argument("--seeds", type=int, default=1_000_000)
     ap.add_argument("--odf-volume", action="store_true",
                     help="time the GPU ODF/PMF volume generation (SH coefficients -> clipped ODF) instead")
+    ap.add_argument("--learned", action="store_true",
+                    help="train and evaluate the learned vMF-mixture proposal instead")
     ap.add_argument("--getter", default="prob", choices=sorted(GETTERS),
                     help="prob = the headline workload; csa/opdt/ptt print supplementary lines")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
@@ -287,9 +289,104 @@ def run_odf_volume(args):
     return 0
 
 
+def run_learned(args):
+    """Learned proposal: trained with the library's CUDA kernels on the plain
+    tracker's steps on one phantom (seed 7), evaluated on the benchmark phantom
+    (seed 1234): NLL, exact-rejection acceptance against the uniform-cone
+    proposal, sampled-distribution check, training and inference throughput."""
+    import torch
+    from scipy.stats import ks_2samp
+
+    from gpustreamlines_b200 import ProbDirectionGetter, Tracker, learned, shm
+    from gpustreamlines_b200.odf import odf_volume_gpu
+    from gpustreamlines_b200.phantom import make_phantom, seeds_from_mask
+    from gpustreamlines_b200.sphere import get_sphere
+
+    sph = get_sphere("repulsion724")
+    cos_max = math.cos(math.radians(45.0))
+
+    def track(seed, nseeds, sseed):
+        ph = make_phantom((81, 106, 76), seed=seed, with_dwi=False)
+        B, _, _ = shm.real_sh_descoteaux(ph.meta["sh_order"], sph.theta, sph.phi)
+        pmf = odf_volume_gpu(ph.sh_coef, B).cpu().numpy()
+        seeds = seeds_from_mask(ph.fa, nseeds, threshold=0.3, seed=sseed).astype(np.float32)
+        with Tracker(ProbDirectionGetter(), pmf, ph.fa, 0.1, sph.vertices, sph.edges,
+                     max_angle=math.radians(45), step_size=0.5) as tr:
+            h = tr.handles[0]
+            h.propagate(seeds)
+            L, S, P = h.fetch()
+        pos, din, dout = learned.steps_from_tracks(L, S, P, seeds)
+        return ph, pmf, pos, din, dout
+
+    t0 = time.time()
+    ph_a, _, pos_a, din_a, dout_a = track(7, 4000, 70)
+    ph_b, pmf_b, pos_b, din_b, dout_b = track(1234, 2000, 1000)
+    prep_s = time.time() - t0
+    net = learned.VmfProposalNet(seed=1)
+    sh_a = learned.trilinear(ph_a.sh_coef, pos_a)
+    f = np.concatenate([sh_a, din_a], axis=1)
+    net.feat_mean = f.mean(0).astype(np.float32)
+    net.feat_std = (f.std(0) + 1e-6).astype(np.float32)
+    Xa = torch.from_numpy(net.features(sh_a, din_a)).cuda()
+    Ta = torch.from_numpy(dout_a.astype(np.float32)).cuda()
+    rng = np.random.default_rng(2)
+    iters, batch = 3000, 1024
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(iters):
+        idx = torch.from_numpy(rng.integers(0, len(pos_a), batch)).cuda()
+        net.train_step(Xa[idx], Ta[idx], lr=2e-3)
+    e1.record()
+    torch.cuda.synchronize()
+    train_ms = e0.elapsed_time(e1)
+    sel = rng.choice(len(pos_b), size=min(3000, len(pos_b)), replace=False)
+    sh_b = learned.trilinear(ph_b.sh_coef, pos_b[sel])
+    Xb = torch.from_numpy(net.features(sh_b, din_b[sel])).cuda()
+    Tb = torch.from_numpy(dout_b[sel].astype(np.float32)).cuda()
+    nll = float(net.loss_and_grad(Xb, Tb).mean())
+    mu, kap, lpi = learned.mixture(net.infer(Xb).cpu().numpy())
+    p, x, cone = learned.target_pmf(pmf_b, sph.vertices, pos_b[sel], din_b[sel], cos_max)
+    ok = p.sum(axis=1) > 0
+    acc_l, acc_u, q = learned.acceptance(p[ok], x[ok], cone[ok], mu[ok], kap[ok], lpi[ok])
+    acc_0, _, _ = learned.acceptance(p[ok], x[ok], cone[ok], mu[ok], kap[ok], lpi[ok], eps=0.0)
+    r = np.random.default_rng(5)
+    a_exact, a_rej, draws = [], [], 0
+    dd = din_b[sel][ok]
+    for b in range(min(2000, int(ok.sum()))):
+        pb, qb, xb = p[ok][b], q[b], x[ok][b]
+        a_exact.append(float(np.dot(xb[r.choice(len(pb), p=pb)], dd[b])))
+        M = np.max(np.divide(pb, qb, out=np.zeros_like(pb), where=pb > 0))
+        for _ in range(100000):
+            v = r.choice(len(qb), p=qb)
+            draws += 1
+            if r.random() * M * qb[v] <= pb[v]:
+                break
+        a_rej.append(float(np.dot(xb[v], dd[b])))
+    Xi = Xb.repeat(max(1, 1_000_000 // len(sel)), 1)
+    net.infer(Xi)
+    _, inf_ms = net.infer(Xi, return_ms=True)
+    print(json.dumps({
+        "workload": "learned vMF-mixture proposal: 48-128-128-128-40 SiLU MLP, trained on the plain prob "
+                    "tracker's steps on phantom seed 7, evaluated on the benchmark phantom (seed 1234)",
+        "train_steps": len(pos_a), "train_iters": iters, "batch": batch,
+        "train_samples_per_s": iters * batch / (train_ms / 1e3),
+        "nll_learned": nll, "nll_uniform_cone": math.log(2 * math.pi * (1 - cos_max)),
+        "nll_uniform_sphere": math.log(4 * math.pi),
+        "acceptance_learned_defensive30": float(acc_l.mean()), "acceptance_learned_bare": float(acc_0.mean()),
+        "acceptance_uniform_cone": float(acc_u.mean()),
+        "rejection_draws_per_step_learned": draws / max(1, len(a_rej)),
+        "ks_turning_angle_exact_vs_rejection_p": float(ks_2samp(a_exact, a_rej).pvalue),
+        "inference_samples_per_s": Xi.shape[0] / (inf_ms / 1e3), "inference_flop_per_sample": 88064,
+        "prep_s": prep_s}), flush=True)
+    return 0
+
+
 def main():
     args = parse()
     rank, world, local = dist_info()
+    if args.learned:
+        return run_learned(args) if rank == 0 else 0
     if args.odf_volume:
         return run_odf_volume(args) if rank == 0 else 0
     if args.impl == "reference":

@@ -66,6 +66,8 @@ EXPORTS = (
     "csl_device_constants", "csl_philox_stream", "csl_last_error", "csl_version",
     "csl_batch_timings", "csl_track_noalloc", "csl_boot_odf", "csl_odf_volume",
     "csl_compress", "csl_fetch_compressed",
+    "csl_mlp_gemm", "csl_mlp_bias_act", "csl_mlp_act_bwd", "csl_mlp_colsum", "csl_mlp_vmf_nll",
+    "csl_mlp_adam", "csl_mlp_param_count", "csl_mlp_infer",
 )
 
 
@@ -99,6 +101,15 @@ def load(path: str | None = None):
     lib.csl_compress.argtypes = [vp, C.POINTER(C.c_double), C.c_double, C.c_double, C.c_int, C.c_int,
                                  C.POINTER(ll)]
     lib.csl_fetch_compressed.argtypes = [vp, _ip, _fp]
+    f32 = C.c_float
+    lib.csl_mlp_gemm.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, vp, C.c_int, vp, C.c_int, vp,
+                                 C.c_int, f32, vp]
+    lib.csl_mlp_bias_act.argtypes = [vp, vp, vp, C.c_int, C.c_int, C.c_int, vp]
+    lib.csl_mlp_act_bwd.argtypes = [vp, vp, vp, ll, vp]
+    lib.csl_mlp_colsum.argtypes = [vp, C.c_int, C.c_int, vp, vp]
+    lib.csl_mlp_vmf_nll.argtypes = [vp, vp, C.c_int, f32, vp, vp, vp]
+    lib.csl_mlp_adam.argtypes = [vp, vp, vp, vp, ll, f32, f32, f32, f32, C.c_int, vp]
+    lib.csl_mlp_infer.argtypes = [vp, vp, C.c_int, vp, _fp, vp]
     lib.csl_odf_volume.argtypes = [vp, ll, C.c_int, vp, C.c_int, C.c_int, vp, vp, ll, _fp, vp]
     lib.csl_philox_stream.argtypes = [C.c_ulonglong, C.c_ulonglong, C.c_ulonglong, ll,
                                       C.POINTER(C.c_uint)]

@@ -259,6 +259,31 @@ int csl_compress(csl_tracker *tracker, const double *affine16, double tol_error,
  * the kept world points [npts_out, 3], streamlines in order. */
 int csl_fetch_compressed(csl_tracker *tracker, int *counts_host, float *points_host);
 
+/*
+ * Learned direction proposal (no counterpart in the reference): kernels of
+ * the 48 -> 128 -> 128 -> 128 -> 40 SiLU MLP that parameterises an 8-component
+ * von Mises-Fisher mixture.  All pointers are device memory, row-major FP32.
+ *   csl_mlp_gemm       C[M,N] = op(A) op(B) (+ beta C), op = transpose when ta / tb
+ *   csl_mlp_bias_act   Z += b per row; A = silu(Z) (act != 0) or Z
+ *   csl_mlp_act_bwd    dZ = dA * silu'(Z)
+ *   csl_mlp_colsum     db[n] = sum over rows of dZ[:, n]
+ *   csl_mlp_vmf_nll    per-sample mixture negative log-likelihood of unit
+ *                      targets X[B,3] and its gradient w.r.t. Y[B,40] (x gscale)
+ *   csl_mlp_adam       Adam step (step >= 1) on n parameters
+ *   csl_mlp_infer      fused inference, weights in shared memory; params in the
+ *                      layout W1 b1 W2 b2 W3 b3 W4 b4 (csl_mlp_param_count floats)
+ */
+int csl_mlp_gemm(int ta, int tb, int M, int N, int K, const float *A, int lda, const float *B, int ldb, float *C,
+                 int ldc, float beta, void *stream);
+int csl_mlp_bias_act(float *Z, const float *b, float *A, int M, int N, int act, void *stream);
+int csl_mlp_act_bwd(const float *Z, const float *dA, float *dZ, long long n, void *stream);
+int csl_mlp_colsum(const float *dZ, int M, int N, float *db, void *stream);
+int csl_mlp_vmf_nll(const float *Y, const float *X, int B, float gscale, float *loss, float *dY, void *stream);
+int csl_mlp_adam(float *p, const float *g, float *m, float *v, long long n, float lr, float b1, float b2, float eps,
+                 int step, void *stream);
+int csl_mlp_param_count(void);
+int csl_mlp_infer(const float *params, const float *X, int B, float *Y, float *ms_out, void *stream);
+
 const char *csl_version(void);
 
 #ifdef __cplusplus

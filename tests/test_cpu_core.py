@@ -164,3 +164,26 @@ def test_boot_fit_option_validation():
         BootDirectionGetter("OPDT", 1.0, *args, fit="bf16x3")
     with pytest.raises(ValueError):
         BootDirectionGetter("CSA", 1.0, *args, fit="tf32")
+
+
+def test_mlp_oracle_gradient_matches_finite_differences():
+    """The float64 restatement of the learned-proposal network (the checker of
+    the CUDA training kernels) is itself pinned by central differences."""
+    from oracle import mlp_ref
+
+    rng = np.random.default_rng(0)
+    n = sum(o * i + o for o, i in mlp_ref.SHAPES)
+    p = rng.normal(size=n) * 0.1
+    X = rng.normal(size=(8, 48))
+    T = rng.normal(size=(8, 3))
+    T /= np.linalg.norm(T, axis=1, keepdims=True)
+    _, g = mlp_ref.grads(p, X, T)
+    eps = 1e-6
+    for k in rng.integers(0, n, 16):
+        q = p.copy()
+        q[k] += eps
+        lp, _ = mlp_ref.grads(q, X, T)
+        q[k] -= 2 * eps
+        lm, _ = mlp_ref.grads(q, X, T)
+        fd = (lp - lm) / (2 * eps)
+        assert abs(fd - g[k]) <= 1e-5 * abs(fd) + 1e-9
