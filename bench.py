@@ -185,8 +185,6 @@ def cpu_baseline(ph, sph, data, seeds, seconds: float, threads: int | None = Non
     from oracle import api
 
     g = GETTERS[getter]
-    if g["model"] == "PTT":
-        raise RuntimeError("the oracle restates the prob and bootstrap getters only")
     threads = threads or os.cpu_count() or 1
     inp = dict(case=dict(model=g["model"], step=0.5, max_angle=g["max_angle"], fa_thr=0.1, rel=0.25,
                          min_sep=45.0, rng_seed=0),
@@ -196,9 +194,17 @@ def cpu_baseline(ph, sph, data, seeds, seconds: float, threads: int | None = Non
     if g["model"] in ("CSA", "OPDT"):
         for k in ("H", "R", "delta_b", "delta_q", "sampling_matrix", "b0s_mask", "min_signal"):
             inp[k] = getattr(dg, k)
+    ptt = None
+    if g["model"] == "PTT":
+        from gpustreamlines_b200.direction_getters import PttDirectionGetter
+
+        pg = PttDirectionGetter()
+        tiled = pg.prepare_data(np.array(data, copy=True), inp["stop_map"], np.float32(0.1), inp["vertices"], False)
+        ptt = dict(tiled=tiled, lut=pg.sphere_vertices_lut_h, log2_x=pg.log2_x, log2_y=pg.log2_y,
+                   nx=pg.nx, ny=pg.ny, nz=pg.nz, res=pg.odf_lut_res)
     ang = np.float32(_m.radians(g["max_angle"]))
-    o = api.Oracle(inp, cos_max_angle=np.float32(_m.cos(ang)))
-    n = 256 if g["model"] == "PROB" else 64
+    o = api.Oracle(inp, cos_max_angle=np.float32(_m.cos(ang)), ptt=ptt)
+    n = {"PROB": 256, "PTT": 16}.get(g["model"], 64)
     steps = 0
     elapsed = 0.0
     used = 0

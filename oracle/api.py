@@ -32,6 +32,10 @@ class OrcParams(C.Structure):
         ("dataf", _fp), ("stop_map", _fp), ("verts", _fp), ("edges", _ip),
         ("H", _fp), ("R", _fp), ("delta_b", _fp), ("delta_q", _fp), ("sampling", _fp),
         ("b0s_mask", _ip),
+        ("ptt_odf", _fp), ("ptt_lut", _fp),
+        ("lut_res", C.c_int), ("log2_x", C.c_int), ("log2_y", C.c_int), ("tile_nx", C.c_int),
+        ("tile_ny", C.c_int), ("tile_nz", C.c_int), ("step_frac", C.c_int), ("ptt_pad", C.c_int),
+        ("probe_step_size", C.c_float), ("probe_quality", C.c_float), ("max_curvature", C.c_double),
     ]
 
 
@@ -109,12 +113,12 @@ def sort_partners():
 class Oracle:
     """Oracle bound to one case's host inputs (see oracle/cases.py)."""
 
-    def __init__(self, inp: dict, cos_max_angle=None, cos_min_sep=None, max_sline_len=501):
+    def __init__(self, inp: dict, cos_max_angle=None, cos_min_sep=None, max_sline_len=501, ptt=None):
         c = inp["case"]
         self.inp = inp
         self._keep = []
         P = OrcParams()
-        model = {"OPDT": 0, "CSA": 1, "PROB": 2}[c["model"]]
+        model = {"OPDT": 0, "CSA": 1, "PROB": 2, "PTT": 3}[c["model"]]
         d = np.ascontiguousarray(inp["dataf"], dtype=np.float32)
         P.model = model
         P.dimx, P.dimy, P.dimz, P.dimt = d.shape
@@ -148,6 +152,20 @@ class Oracle:
             P.b0s_mask = _i(b0)
             P.delta_nr = mats[2].shape[0]
             P.min_signal = float(inp.get("min_signal", 1.0))
+        if model == 3:
+            if ptt is None:
+                raise ValueError("the PTT oracle needs the tiled texture layout (cases.ptt_layout)")
+            tiled = np.ascontiguousarray(ptt["tiled"], dtype=np.float32)
+            lut = np.ascontiguousarray(ptt["lut"], dtype=np.float32)
+            arrs += [tiled, lut]
+            P.ptt_odf, P.ptt_lut = _f(tiled), _f(lut)
+            P.lut_res = int(ptt["res"])
+            P.log2_x, P.log2_y = int(ptt["log2_x"]), int(ptt["log2_y"])
+            P.tile_nx, P.tile_ny, P.tile_nz = int(ptt["nx"]), int(ptt["ny"]), int(ptt["nz"])
+            P.step_frac = int(np.round(np.float32(c["step"]) / 0.025))
+            P.probe_step_size = 0.25
+            P.probe_quality = 8.0
+            P.max_curvature = float(8.0 * np.sin(np.float32(math.radians(c["max_angle"])) / 2.0))
         self._keep = arrs
         self.P = P
 

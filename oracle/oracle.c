@@ -25,6 +25,12 @@
  *   tracker_d / genStreamlinesMergeProb_k generate_streamlines_cuda.cu:283-622
  *   get_direction_boot_d and helpers      boot.cu:20-608
  *   tracker_boot_d / genStreamlinesMergeBoot_k boot.cu:725-980
+ *   get_direction_ptt_d, init_frame_ptt_d, PTT helpers  ptt.cu:1-474
+ *   getNumStreamlinesPtt_k                ptt_init.cu:5-63
+ * The PTT restatement emulates the tiled ODF texture (linear filter, clamp,
+ * 8-bit fractional weights) and the nearest-vertex LUT (point filter,
+ * normalised coordinates), and evaluates sin/cos/rsqrt in libm, so its
+ * streamlines agree with the device's statistically, not bitwise.
  */
 #include <float.h>
 #include <math.h>
@@ -39,9 +45,14 @@
 #include <pmmintrin.h>
 #endif
 
+#ifndef M_PI
+#define M_PI 3.14159265358979323846
+#endif
+
 #define OPDT 0
 #define CSA 1
 #define PROB 2
+#define PTT 3
 
 typedef struct {
     int model;
@@ -60,6 +71,12 @@ typedef struct {
     const int *edges;       /* [E,2] */
     const float *H, *R, *delta_b, *delta_q, *sampling;
     const int *b0s_mask;
+    /* PTT */
+    const float *ptt_odf;  /* tiled texture data [nz*Z][ny*Y][nx*X] */
+    const float *ptt_lut;  /* nearest-vertex index [res][res][res], as float */
+    int lut_res, log2_x, log2_y, tile_nx, tile_ny, tile_nz, step_frac, ptt_pad;
+    float probe_step_size, probe_quality;
+    double max_curvature;
 } orc_params;
 
 static void set_ftz(void) {
@@ -594,6 +611,333 @@ static int boot_get_direction(const orc_params *P, philox_t *lanes, int nattempt
     return 0;
 }
 
+/* ------------------------------------------------------------------- PTT */
+
+#define DISC_V 24
+#define DISC_F 31
+/* disc triangulation at sampling quality 2 (data from nibrary, BSD-3) */
+static const float disc_vert[DISC_V * 2] = {
+    -0.99680788f, -0.07983759f, -0.94276539f, 0.33345677f, -0.87928469f, -0.47629658f,
+    -0.72856617f, 0.68497542f,  -0.60006556f, -0.79995082f, -0.54129995f, -0.02761342f,
+    -0.39271207f, 0.37117272f,  -0.39217391f, 0.91989110f,  -0.36362884f, -0.40757367f,
+    -0.22391316f, -0.97460910f, -0.00130022f, 0.53966106f,  0.00000000f,  0.00000000f,
+    0.00973999f,  0.99995257f,  0.01606516f,  -0.54289908f, 0.21342395f,  -0.97695968f,
+    0.38192071f,  -0.38666136f, 0.38897094f,  0.37442837f,  0.40696681f,  0.91344295f,
+    0.54387161f,  -0.01477123f, 0.59119367f,  -0.80652963f, 0.73955688f,  0.67309406f,
+    0.87601150f,  -0.48229022f, 0.94617928f,  0.32364298f,  0.99585368f,  -0.09096944f};
+static const int disc_face[DISC_F * 3] = {
+    9,  8,  4,  11, 16, 10, 5,  8,  11, 5,  1,  0,  18, 16, 11, 11, 15, 18, 13, 8,  9,
+    11, 8,  13, 13, 15, 11, 22, 18, 23, 22, 20, 16, 16, 18, 22, 16, 20, 17, 12, 10, 17,
+    17, 10, 16, 15, 19, 21, 23, 18, 21, 21, 18, 15, 2,  4,  8,  2,  5,  0,  8,  5,  2,
+    7,  10, 12, 6,  7,  3,  10, 7,  6,  3,  1,  6,  1,  5,  6,  11, 10, 6,  6,  5,  11,
+    14, 19, 15, 15, 13, 14, 14, 13, 9};
+#define PTT_TRIES 1024
+#define K_SMALL 0.0001f
+
+typedef struct {
+    philox_t g;
+    float cached;
+    int has_cached;
+} pttrng_t;
+
+static void pttrng_init(pttrng_t *r, uint64_t seed, uint64_t subseq) {
+    philox_init(&r->g, seed, subseq, 0);
+    r->has_cached = 0;
+    r->cached = 0.0f;
+}
+
+/* Box-Muller, the sine value first and the cosine value cached */
+static float pttrng_normal(pttrng_t *r) {
+    if (r->has_cached) {
+        r->has_cached = 0;
+        return r->cached;
+    }
+    const float u1 = fmaf((float)philox_next(&r->g), 2.3283064365386963e-10f, 2.3283064365386963e-10f / 2.0f);
+    const float u2 = fmaf((float)philox_next(&r->g), 2.3283064365386963e-10f, 2.3283064365386963e-10f / 2.0f);
+    const float rr = sqrtf(-2.0f * logf(u1));
+    const double a = 2.0 * M_PI * (double)u2;
+    r->cached = rr * (float)cos(a);
+    r->has_cached = 1;
+    return rr * (float)sin(a);
+}
+
+static float ptt_texel(const orc_params *P, long long ix, long long iy, long long iz) {
+    const long long W = (long long)P->tile_nx * P->dimx, H = (long long)P->tile_ny * P->dimy,
+                    D = (long long)P->tile_nz * P->dimz;
+    ix = ix < 0 ? 0 : (ix >= W ? W - 1 : ix);
+    iy = iy < 0 ? 0 : (iy >= H ? H - 1 : iy);
+    iz = iz < 0 ? 0 : (iz >= D ? D - 1 : iz);
+    return P->ptt_odf[(iz * H + iy) * W + ix];
+}
+
+/* tiled ODF texture: unnormalised, clamp, linear with 8-bit fractional weights */
+static float tex_odf(const orc_params *P, float x, float y, float z) {
+    const float cx = x - 0.5f, cy = y - 0.5f, cz = z - 0.5f;
+    const float fx = floorf(cx), fy = floorf(cy), fz = floorf(cz);
+    const float ax = rintf((cx - fx) * 256.0f) / 256.0f;
+    const float ay = rintf((cy - fy) * 256.0f) / 256.0f;
+    const float az = rintf((cz - fz) * 256.0f) / 256.0f;
+    const long long ix = (long long)fx, iy = (long long)fy, iz = (long long)fz;
+    float acc = 0.0f;
+    for (int k = 0; k < 2; k++)
+        for (int j = 0; j < 2; j++)
+            for (int i = 0; i < 2; i++) {
+                const float w = (i ? ax : 1.0f - ax) * (j ? ay : 1.0f - ay) * (k ? az : 1.0f - az);
+                acc += w * ptt_texel(P, ix + i, iy + j, iz + k);
+            }
+    return acc;
+}
+
+/* nearest-vertex LUT: normalised coordinates (u fastest), point filter, clamp */
+static float tex_lut(const orc_params *P, float u, float v, float w) {
+    const int n = P->lut_res;
+    long long iu = (long long)floorf(u * n), iv = (long long)floorf(v * n), iw = (long long)floorf(w * n);
+    iu = iu < 0 ? 0 : (iu >= n ? n - 1 : iu);
+    iv = iv < 0 ? 0 : (iv >= n ? n - 1 : iv);
+    iw = iw < 0 ? 0 : (iw >= n ? n - 1 : iw);
+    return P->ptt_lut[(iw * n + iv) * n + iu];
+}
+
+static float interp4(const orc_params *P, const float pos[3], const float *frame) {
+    const float u = fmaf(frame[0], 0.5f, 0.5f), v = fmaf(frame[1], 0.5f, 0.5f), w = fmaf(frame[2], 0.5f, 0.5f);
+    const int idx = (int)tex_lut(P, w, v, u);
+    const int tx = idx & (P->tile_nx - 1);
+    const int ty = (idx >> P->log2_x) & (P->tile_ny - 1);
+    const int tz = idx >> (P->log2_x + P->log2_y);
+    return tex_odf(P, (float)(tx * P->dimx) + pos[0], (float)(ty * P->dimy) + pos[1],
+                   (float)(tz * P->dimz) + pos[2]);
+}
+
+static void norm3(float *x, int fail) {
+    const double n2 = (double)x[0] * x[0] + (double)x[1] * x[1] + (double)x[2] * x[2];
+    const float inv = (float)(1.0 / sqrt(n2));
+    if (isfinite(inv) && inv > 0.0f && inv < 1e8f) {
+        x[0] *= inv; x[1] *= inv; x[2] *= inv;
+    } else {
+        x[0] = x[1] = x[2] = 0;
+        x[fail] = 1.0f;
+    }
+}
+
+static void crossnorm3(float *d, const float *a, const float *b, int fail) {
+    d[0] = a[1] * b[2] - a[2] * b[1];
+    d[1] = a[2] * b[0] - a[0] * b[2];
+    d[2] = a[0] * b[1] - a[1] * b[0];
+    norm3(d, fail);
+}
+
+static void prepare_propagator(float k1, float k2, float arclength, float *pr) {
+    if (fabsf(k1) < K_SMALL && fabsf(k2) < K_SMALL) {
+        pr[0] = arclength; pr[1] = 0; pr[2] = 0; pr[3] = 1; pr[4] = 0; pr[5] = 0; pr[6] = 0; pr[7] = 0; pr[8] = 1;
+        return;
+    }
+    if (fabsf(k1) < K_SMALL) k1 = K_SMALL;
+    if (fabsf(k2) < K_SMALL) k2 = K_SMALL;
+    const float k = sqrtf(k1 * k1 + k2 * k2);
+    const float sinkt = sinf(k * arclength), coskt = cosf(k * arclength);
+    const float kk = 1 / (k * k);
+    pr[0] = sinkt / k;
+    pr[1] = k1 * (1 - coskt) * kk;
+    pr[2] = k2 * (1 - coskt) * kk;
+    pr[3] = coskt;
+    pr[4] = k1 * sinkt / k;
+    pr[5] = k2 * sinkt / k;
+    pr[6] = -pr[5];
+    pr[7] = k1 * k2 * (coskt - 1) * kk;
+    pr[8] = (k1 * k1 + k2 * k2 * coskt) * kk;
+}
+
+static void random_normal(pttrng_t *r, float *pf) {
+    pf[3] = pttrng_normal(r);
+    pf[4] = pttrng_normal(r);
+    pf[5] = pttrng_normal(r);
+    const float dot = pf[3] * pf[0] + pf[4] * pf[1] + pf[5] * pf[2];
+    pf[3] -= dot * pf[0];
+    pf[4] -= dot * pf[1];
+    pf[5] -= dot * pf[2];
+    const float n2 = pf[3] * pf[3] + pf[4] * pf[4] + pf[5] * pf[5];
+    if (n2 < 1e-8f) {
+        const float ax = fabsf(pf[0]), ay = fabsf(pf[1]), az = fabsf(pf[2]);
+        if (ax <= ay && ax <= az) { pf[3] = 0.0f; pf[4] = pf[2]; pf[5] = -pf[1]; }
+        else if (ay <= az) { pf[3] = -pf[2]; pf[4] = 0.0f; pf[5] = pf[0]; }
+        else { pf[3] = pf[1]; pf[4] = -pf[0]; pf[5] = 0.0f; }
+    }
+}
+
+static void probing_frame(int init, const float *frame, pttrng_t *r, float *pf) {
+    if (init) {
+        for (int i = 0; i < 3; i++) pf[i] = frame[i];
+        norm3(pf, 0);
+        random_normal(r, pf);
+        norm3(pf + 3, 1);
+        crossnorm3(pf + 6, pf, pf + 3, 2);
+    } else {
+        for (int i = 0; i < 9; i++) pf[i] = frame[i];
+    }
+}
+
+static void propagate_frame(const float *pr, float *frame, float *direc) {
+    float tmp[3];
+    for (int i = 0; i < 3; i++) {
+        direc[i] = pr[0] * frame[i] + pr[1] * frame[3 + i] + pr[2] * frame[6 + i];
+        tmp[i] = pr[3] * frame[i] + pr[4] * frame[3 + i] + pr[5] * frame[6 + i];
+        frame[6 + i] = pr[6] * frame[i] + pr[7] * frame[3 + i] + pr[8] * frame[6 + i];
+    }
+    norm3(tmp, 0);
+    crossnorm3(frame + 3, frame + 6, tmp, 1);
+    crossnorm3(frame + 6, tmp, frame + 3, 2);
+    for (int i = 0; i < 3; i++) frame[i] = tmp[i];
+}
+
+static float data_support(const orc_params *P, float support, const float pos[3], float k1, float k2, float *pf) {
+    float pr[9], direc[3];
+    float pp[3] = {pos[0], pos[1], pos[2]};
+    prepare_propagator(k1, k2, P->probe_step_size, pr);
+    for (int i = 0; i < (int)P->probe_quality; i++) {
+        propagate_frame(pr, pf, direc);
+        pp[0] += direc[0]; pp[1] += direc[1]; pp[2] += direc[2];
+        support += interp4(P, pp, pf);
+    }
+    return support;
+}
+
+/* get_direction_ptt_d for one warp: lanes[32] generators, frame[9] shared */
+static int ptt_get_direction(const orc_params *P, pttrng_t *lanes, int init, const float dir[3], float *frame,
+                             const float pos[3], float newdir[3]) {
+    if (init) { frame[0] = dir[0]; frame[1] = dir[1]; frame[2] = dir[2]; }
+    const float first_val = interp4(P, pos, frame);
+    const double thr = (double)P->probe_quality * P->pmf_threshold;
+    float vert_pdf[DISC_V], face_cdf[32];
+    int found = 0;
+    for (int ii = 0; ii < DISC_V; ii++) {
+        float pf[9];
+        const float k1 = (float)(disc_vert[2 * ii] * P->max_curvature);
+        const float k2 = (float)(disc_vert[2 * ii + 1] * P->max_curvature);
+        probing_frame(init, frame, &lanes[ii], pf);
+        const float sup = data_support(P, first_val, pos, k1, k2, pf);
+        if ((double)sup < thr) vert_pdf[ii] = 0;
+        else { vert_pdf[ii] = sup; found = 1; }
+    }
+    if (!found) return 0;
+    for (int ii = 0; ii < DISC_F; ii++) {
+        face_cdf[ii] = 0;
+        for (int jj = 0; jj < 3; jj++) {
+            const float v = vert_pdf[disc_face[3 * ii + jj]];
+            if (v == 0) { face_cdf[ii] = 0; break; }
+            face_cdf[ii] += v;
+        }
+    }
+    scan_ref(face_cdf, DISC_F);
+    const float last = face_cdf[DISC_F - 1];
+    if (last == 0) return 0;
+    for (int it = 0; it < PTT_TRIES / 32; it++) {
+        float sup[32], k1s[32], k2s[32], pfs[32][9];
+        for (int l = 0; l < 32; l++) {
+            float r1 = fmaf((float)philox_next(&lanes[l].g), 2.3283064365386963e-10f, 2.3283064365386963e-10f / 2.0f);
+            float r2 = fmaf((float)philox_next(&lanes[l].g), 2.3283064365386963e-10f, 2.3283064365386963e-10f / 2.0f);
+            if (r1 + r2 > 1) { r1 = 1 - r1; r2 = 1 - r2; }
+            const float tmp = fmaf((float)philox_next(&lanes[l].g), 2.3283064365386963e-10f,
+                                   2.3283064365386963e-10f / 2.0f) * last;
+            int jj;
+            for (jj = 0; jj < DISC_F - 1; jj++)
+                if (face_cdf[jj] >= tmp) break;
+            const double mc = P->max_curvature;
+            const float vx0 = (float)(mc * disc_vert[disc_face[jj * 3] * 2]);
+            const float vx1 = (float)(mc * disc_vert[disc_face[jj * 3 + 1] * 2]);
+            const float vx2 = (float)(mc * disc_vert[disc_face[jj * 3 + 2] * 2]);
+            const float vy0 = (float)(mc * disc_vert[disc_face[jj * 3] * 2 + 1]);
+            const float vy1 = (float)(mc * disc_vert[disc_face[jj * 3 + 1] * 2 + 1]);
+            const float vy2 = (float)(mc * disc_vert[disc_face[jj * 3 + 2] * 2 + 1]);
+            k1s[l] = vx0 + r1 * (vx1 - vx0) + r2 * (vx2 - vx0);
+            k2s[l] = vy0 + r1 * (vy1 - vy0) + r2 * (vy2 - vy0);
+            probing_frame(init, frame, &lanes[l], pfs[l]);
+            sup[l] = data_support(P, first_val, pos, k1s[l], k2s[l], pfs[l]);
+        }
+        int win = -1;
+        if (init) {
+            float mx = sup[0];
+            for (int l = 1; l < 32; l++) mx = fmaxf(mx, sup[l]);
+            if ((double)mx >= thr)
+                for (int l = 0; l < 32; l++)
+                    if (sup[l] == mx) { win = l; break; }
+        } else {
+            for (int l = 0; l < 32; l++)
+                if ((double)sup[l] >= thr) { win = l; break; }
+        }
+        if (win >= 0) {
+            newdir[0] = dir[0]; newdir[1] = dir[1]; newdir[2] = dir[2];
+            float *pf = pfs[win];
+            if (!init) {
+                float pr[9], d3[3];
+                prepare_propagator(k1s[win], k2s[win], (float)(P->step_size / P->step_frac), pr);
+                probing_frame(0, frame, &lanes[win], pf);
+                propagate_frame(pr, pf, d3);
+                norm3(d3, 0);
+                newdir[0] = d3[0]; newdir[1] = d3[1]; newdir[2] = d3[2];
+            }
+            for (int q = 0; q < 9; q++) frame[q] = pf[q];
+            return 1;
+        }
+    }
+    return 0;
+}
+
+/* init_frame_ptt_d: frame[0..8] backward, frame[9..17] forward (forward
+ * binormal = backward binormal, as the device library sets it) */
+static int ptt_init_frame(const orc_params *P, pttrng_t *lanes, const float fs[3], const float seed[3],
+                          float *frame) {
+    float tmp[3];
+    int ok = ptt_get_direction(P, lanes, 1, fs, frame, seed, tmp);
+    if (!ok) {
+        const float nfs[3] = {-fs[0], -fs[1], -fs[2]};
+        ok = ptt_get_direction(P, lanes, 1, nfs, frame, seed, tmp);
+        if (!ok) return 0;
+    } else {
+        for (int i = 0; i < 6; i++) frame[i] = -frame[i];
+    }
+    for (int i = 0; i < 6; i++) frame[9 + i] = -frame[i];
+    for (int i = 6; i < 9; i++) frame[9 + i] = frame[i];
+    return 1;
+}
+
+/* getNumStreamlinesPtt_k: ODF at the seed from the tiled texture */
+static int ptt_seed_peaks(const orc_params *P, const float seed[3], float *odf, int *ind) {
+    const int T = P->dimt;
+    for (int i = 0; i < T; i++) {
+        const int tx = i & (P->tile_nx - 1);
+        const int ty = (i >> P->log2_x) & (P->tile_ny - 1);
+        const int tz = i >> (P->log2_x + P->log2_y);
+        float v = tex_odf(P, (float)(tx * P->dimx) + seed[0], (float)(ty * P->dimy) + seed[1],
+                          (float)(tz * P->dimz) + seed[2]);
+        if ((double)v < P->pmf_threshold) v = 0.0f;
+        odf[i] = v;
+    }
+    return peak_directions(P, odf, T, ind);
+}
+
+/* PTT tracking of one direction with step_frac sub-steps per stored point */
+static int ptt_track_one(const orc_params *P, pttrng_t *lanes, const float seed[3], const float d0[3],
+                         float *frame, float *out) {
+    const int sf = P->step_frac;
+    const double ss = P->step_size / sf;
+    float pt[3] = {seed[0], seed[1], seed[2]};
+    float dir[3] = {d0[0], d0[1], d0[2]};
+    out[0] = pt[0]; out[1] = pt[1]; out[2] = pt[2];
+    const int imax = P->max_sline_len * sf;
+    int i;
+    for (i = 1; i < imax; i++) {
+        float nd[3];
+        if (!ptt_get_direction(P, lanes, 0, dir, frame, pt, nd)) break;
+        dir[0] = nd[0]; dir[1] = nd[1]; dir[2] = nd[2];
+        for (int a = 0; a < 3; a++) pt[a] = (float)fma((double)dir[a], ss, (double)pt[a]);
+        if (i % sf == 0) { out[3 * (i / sf)] = pt[0]; out[3 * (i / sf) + 1] = pt[1]; out[3 * (i / sf) + 2] = pt[2]; }
+        if (check_point(P, pt) != TRACKPOINT) break;
+    }
+    int n = i / sf;
+    if ((i % sf) != 0 && i < sf * (P->max_sline_len - 1)) n++;
+    return n;
+}
+
 /* --------------------------------------------------------------- tracker */
 
 typedef struct {
@@ -620,6 +964,7 @@ static void ws_free(ws_t *w) {
 
 static int seed_peaks(const orc_params *P, const float seed[3], long long slid, ws_t *w) {
     if (P->model == PROB) return prob_seed_peaks(P, seed, w->odf, w->ind);
+    if (P->model == PTT) return ptt_seed_peaks(P, seed, w->odf, w->ind);
     for (int l = 0; l < 32; l++) philox_init(&w->lanes[l], P->rng_seed, 32ull * slid + l, 0);
     float unused[3];
     const float zero[3] = {0, 0, 0};
@@ -697,18 +1042,34 @@ long long orc_track(const orc_params *P, const float *seeds, long long n, const 
         ws_alloc(&w, P);
         float *bufB = (float *)malloc(sizeof(float) * 3 * P->max_sline_len);
         float *bufF = (float *)malloc(sizeof(float) * 3 * P->max_sline_len);
+        pttrng_t plane[32];
+        float frame[18];
 #ifdef _OPENMP
 #pragma omp for schedule(dynamic, 4)
 #endif
         for (long long s = 0; s < n; s++) {
             const float *seed = seeds + 3 * s;
             for (int l = 0; l < 32; l++) philox_init(&w.lanes[l], P->rng_seed, 32ull * s + l + 1, 0);
+            if (P->model == PTT)
+                for (int l = 0; l < 32; l++) pttrng_init(&plane[l], P->rng_seed, 32ull * s + l + 1);
             for (int k = 0; k < counts[s]; k++) {
                 const int pv = peaks[s * maxp + k];
                 const float *fs = P->verts + 3 * pv;
                 const float back[3] = {-fs[0], -fs[1], -fs[2]};
-                const int nB = track_one(P, &w, seed, back, bufB);
-                const int nF = track_one(P, &w, seed, fs, bufF);
+                int nB, nF;
+                if (P->model == PTT) {
+                    if (!ptt_init_frame(P, plane, fs, seed, frame)) {
+                        bufB[0] = seed[0]; bufB[1] = seed[1]; bufB[2] = seed[2];
+                        nB = 1;
+                        nF = 1;
+                    } else {
+                        nB = ptt_track_one(P, plane, seed, back, frame, bufB);
+                        nF = ptt_track_one(P, plane, seed, fs, frame + 9, bufF);
+                    }
+                } else {
+                    nB = track_one(P, &w, seed, back, bufB);
+                    nF = track_one(P, &w, seed, fs, bufF);
+                }
                 const long long j = off[s] + k;
                 const int len = nB - 1 + nF;
                 lens[j] = len;

@@ -59,3 +59,40 @@ def test_oracle_reproduces_reference_boot_pass1():
         c, _ = o.seed_peaks(g["seeds"])
         # libm logf vs the kernels' __logf: peak counts agree on nearly all seeds
         assert (c == g["counts"]).mean() >= 0.97
+
+
+def test_oracle_reproduces_reference_ptt_statistics():
+    """PTT restatement vs the reference's own PTT kernels (golden fixture made
+    on a B200): pass-1 peak counts equal on nearly all seeds (the texture
+    filter is emulated), the same streamline count, and backward-half length
+    distributions that agree (libm sin/cos/rsqrt vs the kernels' fast
+    intrinsics change individual curvature draws, not the statistics)."""
+    from scipy.stats import ks_2samp
+
+    from oracle import api, cases
+
+    g = golden("ref_ptt_s.npz")
+    fm = golden("fastmath.npz")
+    angles = list(np.round(np.degrees(fm["angle"])))
+    cos60 = float(fm["cos"][angles.index(60.0)])
+    cos45 = float(fm["cos"][angles.index(45.0)])
+    o = api.Oracle(cases.inputs("ptt_s"), cos_max_angle=cos60, cos_min_sep=cos45, ptt=cases.ptt_layout("ptt_s"))
+    c, L, S, P = o.track(g["seeds"], threads=4)
+    assert (c == g["counts"]).mean() >= 0.95
+    assert abs(len(L) - len(g["lens"])) <= 0.05 * len(g["lens"])
+
+    # backward halves only: the reference leaves the forward frame's binormal
+    # unset (ptt.cu:464-468), so its forward halves follow other frames
+    def backward_lengths(lens, sidx, pts, seeds):
+        off = np.concatenate([[0], np.cumsum(lens)])
+        out = []
+        for i in range(len(lens)):
+            hit = np.nonzero(np.all(pts[off[i]:off[i + 1]] == seeds[sidx[i]], axis=1))[0]
+            if len(hit):
+                out.append(int(hit[0]) + 1)
+        return np.asarray(out)
+
+    b_orc = backward_lengths(L, S, P, g["seeds"])
+    b_ref = backward_lengths(g["lens"], g["sidx"], g["pts"], g["seeds"])
+    assert abs(b_orc.mean() - b_ref.mean()) <= 0.15 * b_ref.mean()
+    assert ks_2samp(b_orc, b_ref).pvalue > 1e-3

@@ -286,6 +286,28 @@ def test_ptt_vs_reference():
     assert p > 1e-3, (p, b0.mean(), b1.mean(), f0.mean(), f1.mean())
 
 
+def test_ptt_vs_oracle():
+    """PTT: the CPU restatement (same fixed forward binormal as the library)
+    against the device kernels over whole streamlines: pass-1 counts equal on
+    >= 95 % of seeds (emulated texture filter), streamline count within 5 %,
+    full and backward-half length distributions agree (KS p > 1e-3)."""
+    from scipy.stats import ks_2samp
+
+    from oracle import api, cases
+
+    seeds = cases.seeds("ptt_s", 600, seed=9)
+    c0, L0, S0, P0, consts = _ours("ptt_s", seeds)
+    o = api.Oracle(cases.inputs("ptt_s"), cos_max_angle=np.float32(consts[0]), cos_min_sep=np.float32(consts[1]),
+                   ptt=cases.ptt_layout("ptt_s"))
+    c1, L1, S1, P1 = o.track(seeds, threads=0)
+    assert (c0 == c1).mean() >= 0.95
+    assert abs(len(L0) - len(L1)) <= 0.05 * len(L0)
+    assert ks_2samp(L0, L1).pvalue > 1e-3, (L0.mean(), L1.mean())
+    b0, _ = _halves(L0, P0, S0, seeds)
+    b1, _ = _halves(L1, P1, S1, seeds)
+    assert ks_2samp(b0, b1).pvalue > 1e-3
+
+
 def test_prob_get_direction_vs_oracle():
     """Per-step directions at fixed (position, direction, Philox state)."""
     from oracle import api, cases
