@@ -67,7 +67,7 @@ EXPORTS = (
     "csl_batch_timings", "csl_track_noalloc", "csl_boot_odf", "csl_odf_volume",
     "csl_compress", "csl_fetch_compressed",
     "csl_mlp_gemm", "csl_mlp_bias_act", "csl_mlp_act_bwd", "csl_mlp_colsum", "csl_mlp_vmf_nll",
-    "csl_mlp_adam", "csl_mlp_param_count", "csl_mlp_infer",
+    "csl_mlp_adam", "csl_mlp_param_count", "csl_mlp_infer", "csl_dti_fa", "csl_seeds_from_mask",
 )
 
 
@@ -110,6 +110,10 @@ def load(path: str | None = None):
     lib.csl_mlp_vmf_nll.argtypes = [vp, vp, C.c_int, f32, vp, vp, vp]
     lib.csl_mlp_adam.argtypes = [vp, vp, vp, vp, ll, f32, f32, f32, f32, C.c_int, vp]
     lib.csl_mlp_infer.argtypes = [vp, vp, C.c_int, vp, _fp, vp]
+    dp = C.POINTER(C.c_double)
+    lib.csl_dti_fa.argtypes = [vp, ll, C.c_int, dp, dp, vp, C.c_double, vp, vp]
+    lib.csl_seeds_from_mask.argtypes = [vp, C.c_int, C.c_int, C.c_int, C.c_float, ll, C.c_ulonglong, vp,
+                                        C.POINTER(ll), vp]
     lib.csl_odf_volume.argtypes = [vp, ll, C.c_int, vp, C.c_int, C.c_int, vp, vp, ll, _fp, vp]
     lib.csl_philox_stream.argtypes = [C.c_ulonglong, C.c_ulonglong, C.c_ulonglong, ll,
                                       C.POINTER(C.c_uint)]

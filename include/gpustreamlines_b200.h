@@ -284,6 +284,22 @@ int csl_mlp_adam(float *p, const float *g, float *m, float *v, long long n, floa
 int csl_mlp_param_count(void);
 int csl_mlp_infer(const float *params, const float *X, int B, float *Y, float *ms_out, void *stream);
 
+/*
+ * The steps before tracking that run_gpu_streamlines.py:289-314 performs on
+ * the host through DIPY, on the device (device pointers; bvals/bvecs host):
+ *   csl_dti_fa           FA from a WLS tensor fit of dwi [nvox, T] (7 <= T <= 512),
+ *                        log signals clamped at min_signal; voxels with
+ *                        mask <= 0 (mask may be NULL) get 0
+ *   csl_seeds_from_mask  n seeds [n, 3] uniform over the voxels of mask
+ *                        [X, Y, Z] above threshold, plus U[-0.5, 0.5)^3 jitter,
+ *                        from Philox streams keyed by seed; *nvox_out = voxels
+ *                        in the mask.  Returns CSL_E_INVALID for an empty mask.
+ */
+int csl_dti_fa(const float *dwi_dev, long long nvox, int T, const double *bvals, const double *bvecs,
+               const float *mask_dev, double min_signal, float *fa_dev, void *stream);
+int csl_seeds_from_mask(const float *mask_dev, int X, int Y, int Z, float threshold, long long n,
+                        unsigned long long seed, float *seeds_dev, long long *nvox_out, void *stream);
+
 const char *csl_version(void);
 
 #ifdef __cplusplus

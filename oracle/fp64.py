@@ -135,3 +135,34 @@ def closest_peak(kept: list[int], verts: np.ndarray, direction: np.ndarray, cos_
     if bdot <= -cos_max:
         return best, -1
     return None
+
+
+def dti_fa_wls(dwi, bvals, bvecs, mask=None, min_signal=1e-6):
+    """FA from the weighted least-squares tensor fit (dipy.reconst.dti WLS:
+    OLS on log signals, weights w = exp(X beta_ols), then the least-squares fit
+    of w X beta = w y), eigenvalues clipped at 0, in float64."""
+    b = np.asarray(bvals, np.float64)
+    g = np.asarray(bvecs, np.float64)
+    X = np.stack([np.ones_like(b), -b * g[:, 0] ** 2, -b * g[:, 1] ** 2, -b * g[:, 2] ** 2,
+                  -2 * b * g[:, 0] * g[:, 1], -2 * b * g[:, 0] * g[:, 2], -2 * b * g[:, 1] * g[:, 2]], 1)
+    P = np.linalg.inv(X.T @ X) @ X.T
+    shp = dwi.shape[:3]
+    y = np.log(np.maximum(np.asarray(dwi, np.float64).reshape(-1, dwi.shape[-1]), min_signal))
+    b0 = y @ P.T
+    w2 = np.exp(b0 @ X.T) ** 2
+    A = np.einsum("nt,ti,tj->nij", w2, X, X)
+    r = np.einsum("nt,ti,nt->ni", w2, X, y)
+    beta = np.linalg.solve(A, r[..., None])[..., 0]
+    D = np.empty((len(beta), 3, 3))
+    D[:, 0, 0], D[:, 1, 1], D[:, 2, 2] = beta[:, 1], beta[:, 2], beta[:, 3]
+    D[:, 0, 1] = D[:, 1, 0] = beta[:, 4]
+    D[:, 0, 2] = D[:, 2, 0] = beta[:, 5]
+    D[:, 1, 2] = D[:, 2, 1] = beta[:, 6]
+    ev = np.clip(np.linalg.eigvalsh(D), 0, None)
+    md = ev.mean(1, keepdims=True)
+    num = np.sqrt(((ev - md) ** 2).sum(1))
+    den = np.sqrt((ev ** 2).sum(1))
+    fa = np.clip(np.sqrt(1.5) * np.where(den > 0, num / np.where(den > 0, den, 1), 0), 0, 1)
+    if mask is not None:
+        fa = np.where(np.asarray(mask).reshape(-1) > 0, fa, 0)
+    return fa.reshape(shp)
