@@ -200,6 +200,59 @@ __device__ __forceinline__ void split8(const float (&x)[8], uint4 &hi, uint4 &lo
     lo = make_uint4(l[0], l[1], l[2], l[3]);
 }
 
+// Tail of the peak search: kept maxima ind[0..n) in ascending vertex order ->
+// descending sort by value (the reference's network), minimum-separation filter.
+__device__ __forceinline__ int peaks_finish(const DevParams &P, const float *odf, int *ind, int n,
+                                            const int *partner_sh, int lane) {
+    const unsigned lmask = (1u << lane) - 1u;
+    if (n == 0) return 0;
+    if (n < kWarp) {
+        float k = -FLT_MAX;
+        int v = 0;
+        if (lane < n) {
+            v = ind[lane];
+            k = odf[v];
+        }
+        warp_sort_desc(partner_sh, lane, k, v);
+        // greedy minimum-separation filter: candidate i is kept unless a
+        // kept peak before it lies within the separation angle
+        const float3 pv = vert3(P.verts, lane < n ? v : 0);
+        unsigned kept = 1u;
+        for (int i = 1; i < n; i++) {
+            const float3 abc = make_float3(__shfl_sync(FULL, pv.x, i), __shfl_sync(FULL, pv.y, i),
+                                           __shfl_sync(FULL, pv.z, i));
+            float cs = abc.x * pv.x + abc.y * pv.y + abc.z * pv.z;
+            if (P.sphere_symm) cs = fabsf(cs);
+            const bool hit = ((kept >> lane) & 1u) && cs > P.cos_min_sep;
+            if (__ballot_sync(FULL, hit) == 0u) kept |= 1u << i;
+        }
+        __syncwarp();
+        if ((kept >> lane) & 1u) ind[__popc(kept & lmask)] = v;
+        __syncwarp();
+        return __popc(kept);
+    }
+    // 32 or more peaks: the reference skips the sort; serial filter on lane 0
+    if (lane == 0) {
+        int k = 1;
+        for (int i = 1; i < n; i++) {
+            const int vi = ind[i];
+            const float3 abc = vert3(P.verts, vi);
+            int j = 0;
+            for (; j < k; j++) {
+                const float3 d = vert3(P.verts, ind[j]);
+                float cs = abc.x * d.x + abc.y * d.y + abc.z * d.z;
+                if (P.sphere_symm) cs = fabsf(cs);
+                if (cs > P.cos_min_sep) break;
+            }
+            if (j == k) ind[k++] = vi;
+        }
+        n = k;
+    }
+    n = __shfl_sync(FULL, n, 0);
+    __syncwarp();
+    return n;
+}
+
 // Peak search of one thresholded ODF row, warp-cooperative, with the
 // semantics of peak_directions_d (tracking_helpers.cu:75-245) and fewer
 // instructions:
@@ -286,52 +339,82 @@ __device__ __forceinline__ int peaks_sparse(const DevParams &P, float *odf, int 
         n += __popc(msk);
     }
     __syncwarp();
-    if (n == 0) return 0;
-    if (n < kWarp) {
-        float k = -FLT_MAX;
-        int v = 0;
-        if (lane < n) {
-            v = ind[lane];
-            k = odf[v];
+    return peaks_finish(P, odf, ind, n, partner_sh, lane);
+}
+
+// Faster exact path of the same search.  A peak is kept only if
+// (value - min) >= RELATIVE_PEAK_THRESH * (max over maxima of value - min);
+// when the arg-max vertex is a strict local maximum that bound is known from
+// one pass, so the local-maximum test runs only on vertices that could be
+// kept (often a minority of the 724), thresholded values computed on the fly.
+// Returns -1 (warp-uniform) when the arg-max is not a strict maximum or the
+// row maximum is not positive; the caller then runs peaks_sparse.
+__device__ __forceinline__ int peaks_fast(const DevParams &P, const float *odf, int *ind, int nr,
+                                          const short *__restrict__ nbr, const int *partner_sh, int lane) {
+    const unsigned lmask = (1u << lane) - 1u;
+    float m = -FLT_MAX, mn = FLT_MAX;
+    int am = 0x7fffffff;
+    for (int v = lane; v < nr; v += kWarp) {
+        const float x = odf[v];
+        if (x > m) {
+            m = x;
+            am = v;
         }
-        warp_sort_desc(partner_sh, lane, k, v);
-        // greedy minimum-separation filter: candidate i is kept unless a
-        // kept peak before it lies within the separation angle
-        const float3 pv = vert3(P.verts, lane < n ? v : 0);
-        unsigned kept = 1u;
-        for (int i = 1; i < n; i++) {
-            const float3 abc = make_float3(__shfl_sync(FULL, pv.x, i), __shfl_sync(FULL, pv.y, i),
-                                           __shfl_sync(FULL, pv.z, i));
-            float cs = abc.x * pv.x + abc.y * pv.y + abc.z * pv.z;
-            if (P.sphere_symm) cs = fabsf(cs);
-            const bool hit = ((kept >> lane) & 1u) && cs > P.cos_min_sep;
-            if (__ballot_sync(FULL, hit) == 0u) kept |= 1u << i;
-        }
-        __syncwarp();
-        if ((kept >> lane) & 1u) ind[__popc(kept & lmask)] = v;
-        __syncwarp();
-        return __popc(kept);
+        mn = fmin_ref(mn, x);
     }
-    // 32 or more peaks: the reference skips the sort; serial filter on lane 0
-    if (lane == 0) {
-        int k = 1;
-        for (int i = 1; i < n; i++) {
-            const int vi = ind[i];
-            const float3 abc = vert3(P.verts, vi);
-            int j = 0;
-            for (; j < k; j++) {
-                const float3 d = vert3(P.verts, ind[j]);
-                float cs = abc.x * d.x + abc.y * d.y + abc.z * d.z;
-                if (P.sphere_symm) cs = fabsf(cs);
-                if (cs > P.cos_min_sep) break;
+#pragma unroll
+    for (int o = 16; o; o >>= 1) {
+        const float om = __shfl_xor_sync(FULL, m, o);
+        const int oa = __shfl_xor_sync(FULL, am, o);
+        if (om > m || (om == m && oa < am)) {
+            m = om;
+            am = oa;
+        }
+        mn = fmin_ref(mn, __shfl_xor_sync(FULL, mn, o));
+    }
+    if (!(m > 0.0f)) return -1;
+    const float thr = (float)(P.pmf_threshold * (double)m);
+    float odf_min = (mn < thr) ? 0.0f : mn;
+    odf_min = (0 > odf_min) ? 0 : odf_min;
+    {
+        float y = m;
+        if (lane < kMaxDegree) {
+            y = odf[nbr[am * kMaxDegree + lane]];
+            y = (y < thr) ? 0.0f : y;
+        }
+        const unsigned larger = __ballot_sync(FULL, m < y), smaller = __ballot_sync(FULL, y < m);
+        if (larger != 0u || smaller == 0u) return -1;
+    }
+    const float mm = m + (-odf_min);
+    const float comp_thres = (float)(P.relative_peak_thresh * (double)mm);
+    int n = 0;
+    for (int j = 0; j < nr; j += kWarp) {
+        const int v = j + lane;
+        bool keep = false;
+        if (v < nr) {
+            float x = odf[v];
+            x = (x < thr) ? 0.0f : x;
+            if ((x - odf_min) >= comp_thres) {
+                const uint4 nb = *reinterpret_cast<const uint4 *>(nbr + v * kMaxDegree);
+                const uint32_t w4[4] = {nb.x, nb.y, nb.z, nb.w};
+                bool larger = false, smaller = false;
+#pragma unroll
+                for (int q = 0; q < 4; q++) {
+                    float y0 = odf[w4[q] & 0xffffu], y1 = odf[w4[q] >> 16];
+                    y0 = (y0 < thr) ? 0.0f : y0;
+                    y1 = (y1 < thr) ? 0.0f : y1;
+                    larger |= (x < y0) | (x < y1);
+                    smaller |= (y0 < x) | (y1 < x);
+                }
+                keep = !larger && smaller;
             }
-            if (j == k) ind[k++] = vi;
         }
-        n = k;
+        const unsigned msk = __ballot_sync(FULL, keep);
+        if (keep) ind[n + __popc(msk & lmask)] = v;
+        n += __popc(msk);
     }
-    n = __shfl_sync(FULL, n, 0);
     __syncwarp();
-    return n;
+    return peaks_finish(P, odf, ind, n, partner_sh, lane);
 }
 
 __device__ __forceinline__ void cp_async16(void *dst, const void *src) {
@@ -733,10 +816,13 @@ __global__ void __launch_bounds__(kBThreads, 1)
                 __syncwarp();
                 float *odf_sh = obuf + buf * g.vstride;
                 const int slot = base + cur;
-                float m = -FLT_MAX;
-                for (int v = lane; v < g.V; v += kWarp) m = fmax_ref(m, odf_sh[v]);
-                m = warp_max_ref(m);
-                const int ndir = peaks_sparse(P, odf_sh, ind_sh, g.V, m, nbr_sh, partner_sh, lane);
+                int ndir = peaks_fast(P, odf_sh, ind_sh, g.V, nbr_sh, partner_sh, lane);
+                if (ndir < 0) {
+                    float m = -FLT_MAX;
+                    for (int v = lane; v < g.V; v += kWarp) m = fmax_ref(m, odf_sh[v]);
+                    m = warp_max_ref(m);
+                    ndir = peaks_sparse(P, odf_sh, ind_sh, g.V, m, nbr_sh, partner_sh, lane);
+                }
                 int found = 0;
                 float3 pk = make_float3(0, 0, 0);
                 if (ndir > 0) {
