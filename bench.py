@@ -83,6 +83,9 @@ GETTERS = {
                              "sh_order 8 (45 coeffs), 81x106x76x160 DWI"),
     "opdt": dict(model="OPDT", max_angle=60.0, sh_order=6,
                  label="bootstrap OPDT getter (plain FP32), sh_order 6 (28 coeffs), 81x106x76x160 DWI"),
+    "opdt_bf16x3": dict(model="OPDT", max_angle=60.0, sh_order=6, fit="bf16x3",
+                        label="bootstrap OPDT getter, batched tensor-core fit (BF16x3, FP32 accumulate), "
+                              "sh_order 6 (28 coeffs), 81x106x76x160 DWI"),
     "ptt": dict(model="PTT", max_angle=60.0,
                 label="PTT getter, 81x106x76 ODF x 724 vertices (tiled texture), step 0.5 = 20 sub-steps"),
 }
@@ -110,7 +113,8 @@ def make_getter(getter: str, ph, sph):
         return BootDirectionGetter.from_dipy_csa(ph.gtab, sph, sh_order_max=g["sh_order"],
                                                  fit=g.get("fit", "fp32"))
     if g["model"] == "OPDT":
-        return BootDirectionGetter.from_dipy_opdt(ph.gtab, sph, sh_order_max=g["sh_order"])
+        return BootDirectionGetter.from_dipy_opdt(ph.gtab, sph, sh_order_max=g["sh_order"],
+                                                  fit=g.get("fit", "fp32"))
     if g["model"] == "PTT":
         return PttDirectionGetter()
     return ProbDirectionGetter()
@@ -524,7 +528,7 @@ def main():
         # the BF16x3 split issues 3x these on the tensor pipe
         nc = dg.delta_nr
         hr = int((dg.b0s_mask == 0).sum())
-        flop = 2 * 2 * hr * hr + 2 * nc * hr + 2 * nc * dg.sampling_matrix.shape[0]
+        flop = 2 * 2 * hr * hr + 2 * nc * hr * (2 if model == "OPDT" else 1) + 2 * nc * dg.sampling_matrix.shape[0]
         tpeak = None
         path = os.path.join(HERE, "MEASURED_PEAKS.json")
         if os.path.exists(path):

@@ -1,4 +1,4 @@
-// Batched residual-bootstrap tracking on the tensor cores (CSA model).
+// Batched residual-bootstrap tracking on the tensor cores (CSA and OPDT models).
 //
 // The plain bootstrap getter (boot.cuh, boot.cu:393-608 in the reference)
 // runs one streamline per warp and streams the fit matrices H, R (150 x 150),
@@ -11,8 +11,8 @@
 //   gather    128 DWI signals (trilinear, non-b0 volumes)       -> A1 [128 x K1]
 //   MMA 1     A1 x [R ; H]^T                                     -> D1 [128 x 2 K1]  (TMEM)
 //   epilogue  h + r[random index], clamp, / b0 mean, CSA
-//             transform log(-log(x))                             -> A2 [128 x K1]
-//   MMA 2     A2 x Delta^T                                       -> D2 [128 x C]     (TMEM)
+//             transform log(-log(x)) or OPDT -log x (1.5+log x) x -> A2 [128 x K1]
+//   MMA 2     A2 x Delta_q^T (OPDT: then += x (-Delta_b)^T)      -> D2 [128 x C]     (TMEM)
 //   epilogue  coefficients (c0 = 1 / (2 sqrt(pi)))               -> A3 [128 x C]
 //   MMA 3     A3 x B^T in 256-vertex chunks                      -> ODF rows         (TMEM -> L2)
 //   peaks     5 % threshold, local maxima, sort, separation,
@@ -83,7 +83,7 @@ BootBatchGeom boot_batch_geom(const DevParams &P, int hr, int nb0) {
 
 __global__ void boot_batch_pack_kernel(DevParams P, BootBatchGeom g, __nv_bfloat16 *B1g,
                                        __nv_bfloat16 *B2g, __nv_bfloat16 *B3g) {
-    const long long n1 = (long long)g.N1 * g.HP, n2 = (long long)g.N2 * g.HP;
+    const long long n1 = (long long)g.N1 * g.HP, n2 = (long long)g.N2 * g.HP * (P.model == OPDT ? 2 : 1);
     const long long n3 = (long long)g.nchunk3 * kOdfChunk * g.N2;
     for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < n1 + n2 + n3;
          e += (long long)gridDim.x * blockDim.x) {
@@ -100,10 +100,15 @@ __global__ void boot_batch_pack_kernel(DevParams P, BootBatchGeom g, __nv_bfloat
             lo = hi + g.b1_chunk / 2;
             off = kmajor_off(n, k % 32, g.N1);
         } else if (e < n1 + n2) {
+            // delta_q, then (OPDT) -delta_b as a second packed operand
             const long long f = e - n1;
-            const int n = (int)(f / g.HP), k = (int)(f % g.HP);
-            x = (n < g.C && k < g.hr) ? P.delta_q[(size_t)n * g.hr + k] : 0.0f;
-            hi = reinterpret_cast<char *>(B2g);
+            const int part = (int)(f / ((long long)g.N2 * g.HP));
+            const long long f2 = f % ((long long)g.N2 * g.HP);
+            const int n = (int)(f2 / g.HP), k = (int)(f2 % g.HP);
+            const float *M = part == 0 ? P.delta_q : P.delta_b;
+            x = (n < g.C && k < g.hr) ? M[(size_t)n * g.hr + k] : 0.0f;
+            if (part == 1) x = -x;
+            hi = reinterpret_cast<char *>(B2g) + (size_t)part * g.b2_bytes;
             lo = hi + g.b2_bytes / 2;
             off = kmajor_off(n, k, g.N2);
         } else {
@@ -640,7 +645,9 @@ __global__ void __launch_bounds__(kBThreads, 1)
         tc_fence_after();
 
         // ---- epilogue 1: residuals to shared memory (this thread's column
-        //      blocks), then bootstrap, clamp, normalise, CSA transform -> A2
+        //      blocks), then bootstrap, clamp, normalise, transform -> A2
+        //      (CSA: log(-log x); OPDT: -log x (1.5 + log x) x, with x itself
+        //      kept in the freed TMEM columns [0, HP) for the second product)
         float *rb = reinterpret_cast<float *>(R0) + (size_t)eslot * (g.hr + 1);
         const int nblk1 = g.HP / 16;
         for (int b = part; b < nblk1; b += 4) {
@@ -662,8 +669,9 @@ __global__ void __launch_bounds__(kBThreads, 1)
                          kBatchSubseqBase + 8ull * (unsigned long long)(sl + A.rng_base) + 4 * half + part, 0);
                 rng_h = h;
             }
+            const bool opdt = P.model == OPDT;
             for (int b = part; b < nblk1; b += 4) {
-                float hv[16];
+                float hv[16], xs[16];
                 tmem_ld16(trow + g.HP + 16 * b, hv);
 #pragma unroll
                 for (int gq = 0; gq < 2; gq++) {
@@ -672,15 +680,22 @@ __global__ void __launch_bounds__(kBThreads, 1)
                     for (int e = 0; e < 8; e++) {
                         const int j = 16 * b + gq * 8 + e;
                         y[e] = 0.0f;
+                        xs[gq * 8 + e] = 0.0f;
                         if (live && j < g.hr) {
                             const int src = pidx ? pidx[j] : (int)(rng.next() % (unsigned)g.hr);
                             float x = hv[gq * 8 + e] + rb[src];
                             x = (P.min_signal > x) ? P.min_signal : x;
                             x = x / denom;
-                            const float lo_c = 0.001f, hi_c = 0.999f;
-                            float cc = (x > lo_c) ? x : lo_c;
-                            cc = (cc < hi_c) ? cc : hi_c;
-                            y[e] = __logf(-__logf(cc));
+                            if (opdt) {
+                                const float ONEP5 = 1.5f;
+                                y[e] = -__logf(x) * (ONEP5 + __logf(x)) * x;
+                                xs[gq * 8 + e] = x;
+                            } else {
+                                const float lo_c = 0.001f, hi_c = 0.999f;
+                                float cc = (x > lo_c) ? x : lo_c;
+                                cc = (cc < hi_c) ? cc : hi_c;
+                                y[e] = __logf(-__logf(cc));
+                            }
                         }
                     }
                     uint4 hi, lo;
@@ -689,6 +704,7 @@ __global__ void __launch_bounds__(kBThreads, 1)
                     *reinterpret_cast<uint4 *>(R1 + off) = hi;
                     *reinterpret_cast<uint4 *>(R1 + a1_term + off) = lo;
                 }
+                if (opdt) tmem_st16(trow + 16 * b, xs);
             }
         }
         fence_async_smem();
@@ -714,6 +730,53 @@ __global__ void __launch_bounds__(kBThreads, 1)
         ph_mma ^= 1;
         tc_fence_after();
 
+        // ---- OPDT: D2 += x (-Delta_b)^T, x back from TMEM into A2 (R1), the
+        //      packed -Delta_b streamed into R0 (the residual buffer is dead)
+        if (P.model == OPDT) {
+            if (t == 0 && ok) {
+                mbar_arrive_expect_tx(&bars[5], (uint32_t)g.b2_bytes);
+                bulk_g2s(R0, A.B2g + g.b2_bytes, (uint32_t)g.b2_bytes, &bars[5]);
+            }
+            for (int b = part; b < g.HP / 16; b += 4) {
+                float xv[16];
+                tmem_ld16(trow + 16 * b, xv);
+#pragma unroll
+                for (int gq = 0; gq < 2; gq++) {
+                    float x[8];
+#pragma unroll
+                    for (int e = 0; e < 8; e++) x[e] = xv[gq * 8 + e];
+                    uint4 hi, lo;
+                    split8(x, hi, lo);
+                    const uint32_t off = kmajor_off(eslot, 16 * b + gq * 8, kSlots);
+                    *reinterpret_cast<uint4 *>(R1 + off) = hi;
+                    *reinterpret_cast<uint4 *>(R1 + a1_term + off) = lo;
+                }
+            }
+            fence_async_smem();
+            tc_fence_before();
+            __syncthreads();
+            if (t == 0 && ok) {
+                ok = mbar_wait(&bars[5], ph_aux);
+                ph_aux ^= 1;
+                if (ok) {
+                    tc_fence_after();
+                    for (int k16 = 0; k16 < g.HP / 16; k16++) {
+#pragma unroll
+                        for (int term = 0; term < 3; term++) {
+                            const uint32_t aoff = (term == 2 ? a1_term : 0) + (uint32_t)(k16 * 2) * (kSlots * 16);
+                            const uint32_t boff = (term == 1 ? b2_term : 0) + (uint32_t)(k16 * 2) * (g.N2 * 16);
+                            umma_bf16(tbase + g.N1, umma_sdesc(smem_u32(R1) + aoff, kSlots * 16, 128),
+                                      umma_sdesc(smem_u32(R0) + boff, g.N2 * 16, 128), idesc2, 1u);
+                        }
+                    }
+                }
+                umma_commit(&bars[4]);
+            }
+            if (!mbar_wait(&bars[4], ph_mma)) ok = false;
+            ph_mma ^= 1;
+            tc_fence_after();
+        }
+
         // ---- epilogue 2: SH coefficients -> A3 (coefficient 0 fixed, boot.cu CSA branch)
         for (int b = part; b < g.N2 / 16; b += 4) {
             float v[16];
@@ -724,7 +787,7 @@ __global__ void __launch_bounds__(kBThreads, 1)
 #pragma unroll
                 for (int e = 0; e < 8; e++) {
                     const int k = 16 * b + gq * 8 + e;
-                    x[e] = (k == 0) ? kN0Const : (k < g.C ? v[gq * 8 + e] : 0.0f);
+                    x[e] = (k == 0 && P.model == CSA) ? kN0Const : (k < g.C ? v[gq * 8 + e] : 0.0f);
                 }
                 uint4 hi, lo;
                 split8(x, hi, lo);

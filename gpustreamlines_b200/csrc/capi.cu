@@ -288,8 +288,6 @@ static int validate(const csl_params *p, const csl_inputs *in, csl_tracker *t) {
                         p->samplm_nr, p->nvertices);
         if (p->boot_fit != 0 && p->boot_fit != 1) return fail(t, CSL_E_INVALID, "boot_fit must be 0 or 1");
         if (p->boot_fit == 1) {
-            if (p->model != CSL_MODEL_CSA)
-                return fail(t, CSL_E_INVALID, "the batched tensor-core fit (boot_fit=1) supports the CSA model");
             if (p->delta_nr > 64) return fail(t, CSL_E_INVALID, "boot_fit=1 supports at most 64 SH coefficients");
             if (p->samplm_nr > 768) return fail(t, CSL_E_INVALID, "boot_fit=1 supports at most 768 sphere samples");
         }
@@ -458,7 +456,7 @@ int csl_create(const csl_params *params, const csl_inputs *inputs, int device, c
                 nbr.resize((size_t)g.nbr_shorts, 0);
                 if ((r = upload(t, t->bb_nbr, nbr.data(), nbr.size()))) return r;
                 CK(t->bb_B1.ensure((size_t)g.nchunk1 * g.b1_chunk));
-                CK(t->bb_B2.ensure((size_t)g.b2_bytes));
+                CK(t->bb_B2.ensure((size_t)g.b2_bytes * (p.model == OPDT ? 2 : 1)));
                 CK(t->bb_B3.ensure((size_t)g.nchunk3 * g.b3_chunk));
                 CK(t->bb_hq.ensure(1));
                 CK(launch_boot_batch_pack(P, g, t->bb_B1.p, t->bb_B2.p, t->bb_B3.p, t->own_stream));
@@ -665,7 +663,7 @@ static int run_batch(csl_tracker *t, const float *seeds_dev, long long n, long l
     CK(t->out_src.ensure((size_t)nsl + 1));
     CK(t->pt_off.ensure((size_t)nsl + 1));
 
-    if (t->hp.boot_fit == 1 && P.model == CSA) {
+    if (t->hp.boot_fit == 1 && (P.model == CSA || P.model == OPDT)) {
         const int r = run_boot_batch(t, seeds_dev, ni, nsl, rng_base, st);
         if (r != kUsePerWarpPath) return r;
     }

@@ -1,7 +1,7 @@
 // Blackwell (sm_100a) tensor-core primitives, hand-written inline PTX:
 // shared-memory mbarriers, 1-D bulk copies global -> shared (no multicast),
 // tensor-memory allocation, tcgen05.mma (kind::f16, BF16 in / FP32 out,
-// both operands in shared memory), tcgen05.commit and tcgen05.ld.
+// both operands in shared memory), tcgen05.commit, tcgen05.ld and tcgen05.st.
 //
 // Operand layout used everywhere in this library: K-major, no swizzle.  The
 // element (row r, k) of a [rows x K] bf16 tile lives at byte
@@ -160,6 +160,21 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
     asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 #pragma unroll
     for (int i = 0; i < 16; i++) v[i] = __uint_as_float(r[i]);
+}
+
+// store 16 consecutive 32-bit columns of this thread's TMEM lane (warp-collective)
+__device__ __forceinline__ void tmem_st16(uint32_t taddr, const float (&v)[16]) {
+    asm volatile(
+        "tcgen05.st.sync.aligned.32x32b.x16.b32 [%0], "
+        "{%1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15, %16};" ::"r"(taddr),
+        "r"(__float_as_uint(v[0])), "r"(__float_as_uint(v[1])), "r"(__float_as_uint(v[2])),
+        "r"(__float_as_uint(v[3])), "r"(__float_as_uint(v[4])), "r"(__float_as_uint(v[5])),
+        "r"(__float_as_uint(v[6])), "r"(__float_as_uint(v[7])), "r"(__float_as_uint(v[8])),
+        "r"(__float_as_uint(v[9])), "r"(__float_as_uint(v[10])), "r"(__float_as_uint(v[11])),
+        "r"(__float_as_uint(v[12])), "r"(__float_as_uint(v[13])), "r"(__float_as_uint(v[14])),
+        "r"(__float_as_uint(v[15]))
+        : "memory");
+    asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
 }
 
 // byte offset of element (r, k) in the K-major no-swizzle layout above

@@ -64,8 +64,6 @@ class BootDirectionGetter(GPUDirectionGetter):
         BF16x3 products and FP32 accumulation."""
         if fit not in ("fp32", "bf16x3"):
             raise ValueError(f"Invalid fit {fit!r}, must be one of 'fp32', 'bf16x3'")
-        if fit == "bf16x3" and model_type.upper() != "CSA":
-            raise ValueError("the batched tensor-core fit (fit='bf16x3') supports the CSA model")
         self.fit = fit
         if model_type.upper() == "OPDT":
             self.model_type = _lib.MODEL_OPDT

@@ -69,7 +69,7 @@ typedef struct csl_params {
     int boot_fit;                 /* bootstrap fit: 0 = one warp per streamline in FP32 with the
                                      reference's arithmetic (results identical to it); 1 = batched
                                      fit on the tensor cores in BF16x3 with FP32 accumulation, 128
-                                     streamline halves per CTA (CSA model; no counterpart in the
+                                     streamline halves per CTA (CSA or OPDT; no counterpart in the
                                      reference, whose getter is the per-warp one, boot.cu:393-608) */
     /* PTT getter (PttDirectionGetter, cu_direction_getters.py:417-468) */
     int odf_lut_res;              /* nearest-vertex LUT resolution (128) */

@@ -152,7 +152,7 @@ def test_phantom_is_deterministic():
 
 
 def test_boot_fit_option_validation():
-    """fit='bf16x3' is the batched tensor-core CSA fit; other models and names are rejected."""
+    """fit='bf16x3' is the batched tensor-core fit (CSA, OPDT); other names are rejected."""
     from gpustreamlines_b200 import BootDirectionGetter
     from oracle import cases
 
@@ -160,8 +160,7 @@ def test_boot_fit_option_validation():
     args = (inp["H"], inp["R"], inp["delta_b"], inp["delta_q"], inp["sampling_matrix"], inp["b0s_mask"])
     assert BootDirectionGetter("CSA", 1.0, *args, fit="bf16x3").fit == "bf16x3"
     assert BootDirectionGetter("CSA", 1.0, *args).fit == "fp32"
-    with pytest.raises(ValueError):
-        BootDirectionGetter("OPDT", 1.0, *args, fit="bf16x3")
+    assert BootDirectionGetter("OPDT", 1.0, *args, fit="bf16x3").fit == "bf16x3"
     with pytest.raises(ValueError):
         BootDirectionGetter("CSA", 1.0, *args, fit="tf32")
 

@@ -26,10 +26,12 @@ from test_gpu_parity import _handle
 pytestmark = pytest.mark.gpu
 
 
-def _inputs(sh_order):
+def _inputs(sh_order, model="CSA"):
     from gpustreamlines_b200 import shm
     from oracle import cases
 
+    if model == "OPDT":
+        return cases.inputs("opdt_s")
     base = cases.inputs("csa_s")
     if sh_order == base["case"]["sh_order"]:
         return base
@@ -42,25 +44,25 @@ def _inputs(sh_order):
     return inp
 
 
-def _measure(sh_order, n=1500, seed=5):
+def _measure(sh_order, n=1500, seed=5, model="CSA"):
     import torch
 
     from gpustreamlines_b200.phantom import seeds_from_mask
     from oracle import fp64
 
-    inp = _inputs(sh_order)
+    inp = _inputs(sh_order, model)
     rng = np.random.default_rng(seed)
     pts = seeds_from_mask(inp["stop_map"], n, threshold=0.2, seed=seed).astype(np.float32)
     hr = int((np.asarray(inp["b0s_mask"]) == 0).sum())
     idx = rng.integers(0, hr, size=(n, hr)).astype(np.int32)
     V = inp["sampling_matrix"].shape[0]
     stride = (V + 3) // 4 * 4
-    ref = fp64.boot_odf(inp, "CSA", pts, idx)
+    ref = fp64.boot_odf(inp, model, pts, idx)
 
     pts_d = torch.from_numpy(pts).cuda()
     idx_d = torch.from_numpy(idx).cuda()
     out = {}
-    h = _handle("csa_s", inp, boot_fit=1)
+    h = _handle("opdt_s" if model == "OPDT" else "csa_s", inp, boot_fit=1)
     try:
         for fit in (0, 1):
             o = torch.empty((n, stride), dtype=torch.float32, device="cuda")
@@ -78,7 +80,7 @@ def _measure(sh_order, n=1500, seed=5):
     dirs /= np.linalg.norm(dirs, axis=1, keepdims=True)
     scale = np.maximum(np.abs(ref).max(axis=1), 1e-30)
     live = np.abs(ref).max(axis=1) > 0
-    rep = {"points": int(live.sum()), "sh_order": sh_order, "n_coef": int(inp["delta_q"].shape[0])}
+    rep = {"model": model, "points": int(live.sum()), "sh_order": sh_order, "n_coef": int(inp["delta_q"].shape[0])}
     steps_ref = [fp64.closest_peak(fp64.peaks(ref[i], verts, edges, 0.25, cos_sep), verts, dirs[i], cos_max)
                  for i in range(n)]
     for fit, name in ((0, "fp32"), (1, "bf16x3")):
@@ -100,9 +102,9 @@ def _measure(sh_order, n=1500, seed=5):
     return rep
 
 
-@pytest.mark.parametrize("sh_order", [6, 8])
-def test_fit_accuracy_vs_float64(sh_order):
-    rep = _measure(sh_order)
+@pytest.mark.parametrize("model,sh_order", [("CSA", 6), ("CSA", 8), ("OPDT", 4)])
+def test_fit_accuracy_vs_float64(model, sh_order):
+    rep = _measure(sh_order, model=model)
     path = os.environ.get("CSL_ACCURACY_OUT")
     if path:
         with open(path, "a") as f:

@@ -33,15 +33,15 @@ def _contains_seed(L, S, P, seeds):
     return all(np.any(np.all(P[off[i]:off[i + 1]] == seeds[S[i]], axis=1)) for i in range(len(L)))
 
 
-@pytest.mark.parametrize("n", [600])
-def test_batched_fit_matches_plain_statistics(n):
+@pytest.mark.parametrize("name", ["csa_s", "opdt_s"])
+def test_batched_fit_matches_plain_statistics(name, n=600):
     from scipy.stats import ks_2samp
 
     from oracle import cases
 
-    seeds = cases.seeds("csa_s", n, seed=11)
-    L0, S0, P0 = _track("csa_s", seeds, "fp32")
-    L1, S1, P1 = _track("csa_s", seeds, "bf16x3")
+    seeds = cases.seeds(name, n, seed=11)
+    L0, S0, P0 = _track(name, seeds, "fp32")
+    L1, S1, P1 = _track(name, seeds, "bf16x3")
     assert len(L0) == len(L1) > 0
     assert np.array_equal(S0, S1)
     assert abs(L1.mean() - L0.mean()) <= 0.03 * L0.mean()
