@@ -126,7 +126,7 @@ class Oracle:
         edges = np.ascontiguousarray(inp["edges"], dtype=np.int32)
         P.nvert, P.nedges = len(verts), len(edges)
         P.samplm_nr = inp["sampling_matrix"].shape[0] if model < 2 else d.shape[3]
-        P.sphere_symm = 0
+        P.sphere_symm = int(c.get("sphere_symm", 0))
         P.max_sline_len = max_sline_len
         P.step_size = float(np.float32(c["step"]))
         P.max_angle = float(np.float32(math.radians(c["max_angle"])))

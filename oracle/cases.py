@@ -32,6 +32,11 @@ CASES = {
     # parallel transport tractography on the small phantom's ODF
     "ptt_s": dict(model="PTT", shape=(24, 28, 20), phantom_seed=7, max_angle=60.0, step=0.5,
                   fa_thr=0.1, rel=0.25, min_sep=45.0, rng_seed=0),
+    # probabilistic getter with other tracker parameters: finer step, narrower
+    # cone, lower relative peak threshold, symmetric-sphere peak separation,
+    # higher stop threshold and a non-zero generator seed
+    "prob_v": dict(model="PROB", shape=(24, 28, 20), phantom_seed=7, max_angle=30.0,
+                   step=0.25, fa_thr=0.2, rel=0.1, min_sep=30.0, rng_seed=77, sphere_symm=1),
     # probabilistic getter at the full 81x106x76x724 size
     "prob_full": dict(model="PROB", shape=(81, 106, 76), phantom_seed=1234, max_angle=45.0,
                       step=0.5, fa_thr=0.1, rel=0.25, min_sep=45.0, rng_seed=0),
@@ -98,7 +103,7 @@ def macros(name):
         "RNG_SEED": str(int(c["rng_seed"])),
         "SAMPLM_NR": str(int(samplm)),
         "NUM_EDGES": str(int(len(inp["edges"]))),
-        "SPHERE_SYMM": "0",
+        "SPHERE_SYMM": str(int(c.get("sphere_symm", 0))),
         "EXCESS_ALLOC_FACT": "2", "MAX_SLINES_PER_SEED": "10",
         "MAX_SLINE_LEN": str(MAX_SLINE_LEN), "PMF_THRESHOLD_P": str(float(0.05)),
         "REAL_SIZE": "4", "THR_X_BL": "64", "THR_X_SL": "32",

@@ -7,7 +7,9 @@ Bars
   * integer outputs -- pass-1 peak counts (hence offsets), seed indices --
     bit-exact against the reference kernels, for all three getters;
   * probabilistic streamlines (lengths and float32 points) bit-exact against
-    the reference kernels; against the oracle, bit-exact except where a stop
+    the reference kernels, for the default parameters and for a variant
+    (step 0.25, 30 deg cone, relative threshold 0.1, 30 deg separation,
+    symmetric sphere, stop 0.2, generator seed 77); against the oracle, bit-exact except where a stop
     decision falls within the oracle's texture-emulation band (< 5e-3);
   * per-step probabilistic directions at fixed (position, direction, Philox
     state) identical to the oracle's;
@@ -52,6 +54,7 @@ def _handle(name, inp=None, seed_order=0, boot_fit=0):
     p.rng_seed = int(c["rng_seed"])
     p.seed_order = seed_order
     p.boot_fit = boot_fit
+    p.sphere_symm = int(c.get("sphere_symm", 0))
     ins = _lib.CslInputs()
     ins.stop_map = _lib.fptr(inp["stop_map"])
     ins.vertices = _lib.fptr(inp["vertices"])
@@ -181,7 +184,7 @@ def test_stop_texture_emulation():
     assert ((hw > 0.1) == (em > 0.1)).mean() > 0.999
 
 
-@pytest.mark.parametrize("name,n", [("prob_s", 2000), ("prob_full", 3000)])
+@pytest.mark.parametrize("name,n", [("prob_s", 2000), ("prob_v", 2000), ("prob_full", 3000)])
 def test_prob_bit_exact_vs_reference(name, n):
     from oracle import cases
 
