@@ -53,6 +53,9 @@ def parse():
     ap.add_argument("--seeds", type=int, default=1_000_000)
     ap.add_argument("--odf-volume", action="store_true",
                     help="time the GPU ODF/PMF volume generation (SH coefficients -> clipped ODF) instead")
+    ap.add_argument("--multi", action="store_true",
+                    help="multi-subject run: uneven subjects, mixed getters, one CUDA-graph launch")
+    ap.add_argument("--subjects", type=int, default=12)
     ap.add_argument("--learned", action="store_true",
                     help="train and evaluate the learned vMF-mixture proposal instead")
     ap.add_argument("--getter", default="prob", choices=sorted(GETTERS),
@@ -299,6 +302,148 @@ def run_odf_volume(args):
     return 0
 
 
+def multi_subjects(nsub: int, seed: int = 5):
+    """Uneven synthetic subjects for the multi-subject run: volumes log-uniform
+    between 48^3 and 96x116x96 voxels (phantom shape scaled), two diffusion
+    schemes (6 b0 + 64 dirs at b=1000, 2.5 mm; 10 b0 + 150 dirs at b=2000,
+    2 mm), seeds log-uniform in [5k, 250k] (a fifth of that for bootstrap
+    and PTT subjects, whose steps cost 15-50x a probabilistic step), getters
+    cycling probabilistic, bootstrap CSA, PTT, probabilistic, bootstrap OPDT,
+    probabilistic."""
+    rng = np.random.default_rng(seed)
+    cycle = ["prob", "csa", "ptt", "prob", "opdt", "prob"]
+    vox = np.exp(rng.uniform(np.log(48 ** 3), np.log(96 * 116 * 96), nsub))
+    nseeds = np.exp(rng.uniform(np.log(5_000), np.log(250_000), nsub)).astype(int)
+    out = []
+    for i in range(nsub):
+        scale = (vox[i] / (81 * 106 * 76)) ** (1 / 3)
+        shape = tuple(max(24, int(round(d * scale))) for d in (81, 106, 76))
+        n_b0, n_dirs, bval, mm = [(6, 64, 1000.0, 2.5), (10, 150, 2000.0, 2.0)][i % 2]
+        getter = cycle[i % len(cycle)]
+        n = int(nseeds[i]) if getter == "prob" else max(1000, int(nseeds[i]) // 5)
+        out.append(dict(getter=getter, shape=shape, n_b0=n_b0, n_dirs=n_dirs, bval=bval,
+                        voxel_mm=mm, seeds=n, seed=100 + i))
+    return out
+
+
+def run_multi(args):
+    """All subjects' batches as one captured CUDA graph (MultiSubjectRun)
+    against the same batches tracked one after another through the plain
+    per-subject path (host round trips between pass 1, pass 2 and compaction)."""
+    import torch
+
+    from gpustreamlines_b200 import Tracker
+    from gpustreamlines_b200.multi import MultiSubjectRun
+    from gpustreamlines_b200.phantom import make_phantom, odf_volume, seeds_from_mask
+    from gpustreamlines_b200.sphere import get_sphere
+
+    sph = get_sphere("repulsion724")
+    subs = multi_subjects(args.subjects)
+    trackers, seeds, vol_bytes = [], [], 0
+    t_setup = time.perf_counter()
+    for sd in subs:
+        g = GETTERS[sd["getter"]]
+        boot = g["model"] in ("CSA", "OPDT")
+        ph = make_phantom(sd["shape"], seed=sd["seed"], n_b0=sd["n_b0"], n_dirs=sd["n_dirs"], bval=sd["bval"],
+                          voxel_mm=sd["voxel_mm"], with_dwi=boot)
+        data = np.ascontiguousarray(ph.dwi, dtype=np.float32) if boot else odf_volume(ph, sph)
+        vol_bytes += data.nbytes
+        dg = make_getter(sd["getter"], ph, sph)
+        tr = Tracker(dg, data, ph.fa, 0.1, sph.vertices, sph.edges, max_angle=math.radians(g["max_angle"]),
+                     step_size=0.5, ngpus=1, device_offset=0)
+        tr.__enter__()
+        trackers.append(tr)
+        seeds.append(seeds_from_mask(ph.fa, sd["seeds"], threshold=0.3, seed=sd["seed"]).astype(np.float32))
+        del data
+    t_setup = time.perf_counter() - t_setup
+    stream = torch.cuda.Stream()
+    run = MultiSubjectRun(trackers, seeds)
+    for _ in range(args.warmup):
+        run.launch(stream.cuda_stream)
+        run.wait()
+    nsl, npts, rep, _ = run.last
+    steps = int((npts - nsl).sum())
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    replays, graph_ms = 0, []
+    torch.cuda.synchronize()
+    with ClockSampler(0) as clk:
+        ev0.record(stream)
+        for _ in range(args.steps):
+            run.launch(stream.cuda_stream)
+            _, _, rep, ms = run.wait()
+            replays += int(rep.sum())
+            graph_ms.append(ms)
+        ev1.record(stream)
+        torch.cuda.synchronize()
+    multi_ms = ev0.elapsed_time(ev1) / args.steps
+    captures, _, _ = run.plan.info()
+
+    # the same batches one after another through the plain path
+    dev = [t for t, _ in run._seeds]
+    handles = [tr.handles[0] for tr in trackers]
+    for h, d, s in zip(handles, dev, seeds):
+        h.propagate_device(d.data_ptr(), len(s), 0, stream.cuda_stream)
+    torch.cuda.synchronize()
+    ev0.record(stream)
+    for _ in range(args.steps):
+        for h, d, s in zip(handles, dev, seeds):
+            h.propagate_device(d.data_ptr(), len(s), 0, stream.cuda_stream)
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    seq_ms = ev0.elapsed_time(ev1) / args.steps
+    seq_steps = sum(h.counts()[1] - h.counts()[0] for h in handles)
+
+    # end to end: seeds from pinned host memory, one graph launch, results to pinned host memory
+    pinned = [torch.from_numpy(s).pin_memory() for s in seeds]
+    outs = [(torch.empty(int(a), dtype=torch.int32).pin_memory().numpy(),
+             torch.empty(int(a), dtype=torch.int32).pin_memory().numpy(),
+             torch.empty((int(b), 3), dtype=torch.float32).pin_memory().numpy()) for a, b in zip(nsl, npts)]
+    torch.cuda.synchronize()
+    ev0.record(stream)
+    for _ in range(args.steps):
+        with torch.cuda.stream(stream):
+            for d, p in zip(dev, pinned):
+                if len(p):
+                    d[: len(p)].copy_(p, non_blocking=True)
+        run.launch(stream.cuda_stream)
+        _, np_, _, _ = run.wait()
+        for h, (L, S, P), k in zip(handles, outs, np_):
+            if len(L) and int(k) == len(P):
+                h.fetch_into(L, S, P)
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = ev0.elapsed_time(ev1) / args.steps
+    h2d = sum(s.nbytes for s in seeds)
+    d2h = sum(L.nbytes + S.nbytes + P.nbytes for L, S, P in outs)
+    run.close()
+    for tr in trackers:
+        tr.__exit__(None, None, None)
+    nonempty = sum(1 for s in seeds if len(s))
+    print(json.dumps({
+        "metric": "tracking steps/s, multi-subject run in one CUDA-graph launch", "value": steps / (multi_ms / 1e3),
+        "unit": "steps/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": multi_ms,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic phantoms (seeded), random seeds in FA>0.3",
+        "config": {"workload": f"{len(subs)} subjects of uneven size, mixed getters, one graph launch",
+                   "subjects": [{k: sd[k] for k in ("getter", "shape", "n_dirs", "seeds")} for sd in subs],
+                   "seeds_total": int(sum(len(s) for s in seeds)), "streamlines_total": int(nsl.sum()),
+                   "steps_total": steps, "volume_bytes_total": vol_bytes,
+                   "l2": "inputs (volumes) larger than L2; no flush", "setup_s": t_setup,
+                   "graph_device_ms": float(np.median(graph_ms)), "graph_captures": captures,
+                   "replays_in_timed_region": replays,
+                   "bootstrap_fit": "per-warp FP32 (the graph path)"},
+        "sequential_plain": {"value": seq_steps / (seq_ms / 1e3), "ms_per_step": seq_ms,
+                             "note": "same batches, one csl_propagate_device per subject in turn"},
+        "speedup_vs_sequential": seq_ms / multi_ms,
+        "e2e": {"value": steps / (e2e_ms / 1e3), "unit": "steps/s", "h2d_bytes_per_step": h2d,
+                "d2h_bytes_per_step": d2h},
+        "roofline": None,
+        "gpu_launches": 7 * nonempty * args.steps,
+        "clocks": clk.summary(),
+    }), flush=True)
+    return 0
+
+
 def run_learned(args):
     """Learned proposal: trained with the library's CUDA kernels on the plain
     tracker's steps on one phantom (seed 7), evaluated on the benchmark phantom
@@ -399,6 +544,8 @@ def main():
         return run_learned(args) if rank == 0 else 0
     if args.odf_volume:
         return run_odf_volume(args) if rank == 0 else 0
+    if args.multi:
+        return run_multi(args) if rank == 0 else 0
     if args.impl == "reference":
         return run_reference(args, rank, world)
 

@@ -68,6 +68,8 @@ EXPORTS = (
     "csl_compress", "csl_fetch_compressed",
     "csl_mlp_gemm", "csl_mlp_bias_act", "csl_mlp_act_bwd", "csl_mlp_colsum", "csl_mlp_vmf_nll",
     "csl_mlp_adam", "csl_mlp_param_count", "csl_mlp_infer", "csl_dti_fa", "csl_seeds_from_mask",
+    "csl_multi_create", "csl_multi_launch", "csl_multi_wait", "csl_multi_info", "csl_multi_destroy",
+    "csl_set_launch", "csl_get_launch", "csl_autotune",
 )
 
 
@@ -117,6 +119,15 @@ def load(path: str | None = None):
     lib.csl_odf_volume.argtypes = [vp, ll, C.c_int, vp, C.c_int, C.c_int, vp, vp, ll, _fp, vp]
     lib.csl_philox_stream.argtypes = [C.c_ulonglong, C.c_ulonglong, C.c_ulonglong, ll,
                                       C.POINTER(C.c_uint)]
+    llp = C.POINTER(ll)
+    lib.csl_multi_create.argtypes = [C.POINTER(vp), C.POINTER(vp), llp, llp, C.c_int, C.c_int, C.POINTER(vp)]
+    lib.csl_multi_launch.argtypes = [vp, vp]
+    lib.csl_multi_wait.argtypes = [vp, llp, llp, _ip, _fp]
+    lib.csl_multi_info.argtypes = [vp, _ip, _ip, llp]
+    lib.csl_multi_destroy.argtypes = [vp]
+    lib.csl_set_launch.argtypes = [vp, C.c_int, C.c_int]
+    lib.csl_get_launch.argtypes = [vp, _ip, _ip, _ip]
+    lib.csl_autotune.argtypes = [vp, vp, ll, ll, C.c_int, _fp]
     lib.csl_last_error.argtypes = [vp, C.c_char_p, C.c_int]
     lib.csl_version.restype = C.c_char_p
     for name in EXPORTS:
@@ -292,7 +303,81 @@ class Handle:
         self._chk(self.lib.csl_batch_timings(self.h, fptr(ms), C.byref(runs)))
         return tuple(float(x) for x in ms), runs.value
 
+    def set_launch(self, threads_per_block: int, seed_order: int):
+        self._chk(self.lib.csl_set_launch(self.h, int(threads_per_block), int(seed_order)))
+
+    def get_launch(self):
+        """(threads per CTA, seed order, CTAs per SM) of the per-warp tracking path."""
+        b, o, k = C.c_int(), C.c_int(), C.c_int()
+        self._chk(self.lib.csl_get_launch(self.h, C.byref(b), C.byref(o), C.byref(k)))
+        return b.value, o.value, k.value
+
+    def autotune(self, seeds_ptr: int, n: int, rng_index_base: int = 0, repeats: int = 2):
+        """Time the six launch shapes on a device seed sample and keep the fastest.
+
+        Returns {(threads_per_block, seed_order): ms or None}."""
+        ms = np.zeros(6, dtype=np.float32)
+        self._chk(self.lib.csl_autotune(self.h, C.c_void_p(seeds_ptr), int(n), int(rng_index_base),
+                                        int(repeats), fptr(ms)))
+        shapes = [(256, 0), (256, 1), (128, 0), (128, 1), (64, 0), (64, 1)]
+        return {sh: (float(v) if v >= 0 else None) for sh, v in zip(shapes, ms)}
+
     def device_constants(self):
         a, b = C.c_float(), C.c_float()
         self._chk(self.lib.csl_device_constants(self.h, C.byref(a), C.byref(b)))
         return a.value, b.value
+
+
+class MultiPlan:
+    """Owns one ``csl_multi``: the batches of several handles (subjects) as
+    branches of one captured CUDA graph.  ``seeds`` are device pointers with
+    their counts; the plan keeps the handles alive."""
+
+    def __init__(self, handles, seeds_ptrs, counts, rng_index_base=None, points_per_streamline: int = 0):
+        self.lib = load()
+        n = len(handles)
+        if not (len(seeds_ptrs) == len(counts) == n):
+            raise ValueError("one seed batch per subject")
+        self.handles = list(handles)
+        self.n = n
+        subs = (C.c_void_p * n)(*[h.h for h in handles])
+        sp = (C.c_void_p * n)(*[int(p) for p in seeds_ptrs])
+        cnt = (C.c_longlong * n)(*[int(c) for c in counts])
+        rb = None if rng_index_base is None else (C.c_longlong * n)(*[int(r) for r in rng_index_base])
+        p = C.c_void_p()
+        check(self.lib.csl_multi_create(subs, sp, cnt, rb, n, int(points_per_streamline), C.byref(p)))
+        self.p = p
+
+    def launch(self, stream: int | None = None):
+        check(self.lib.csl_multi_launch(self.p, C.c_void_p(stream) if stream else None))
+
+    def wait(self):
+        """(n_streamlines [n], n_points [n], replayed [n], graph ms)."""
+        nsl = np.zeros(self.n, dtype=np.int64)
+        npts = np.zeros(self.n, dtype=np.int64)
+        rep = np.zeros(self.n, dtype=np.int32)
+        ms = np.zeros(1, dtype=np.float32)
+        llp = C.POINTER(C.c_longlong)
+        check(self.lib.csl_multi_wait(self.p, nsl.ctypes.data_as(llp), npts.ctypes.data_as(llp), iptr(rep),
+                                      fptr(ms)))
+        return nsl, npts, rep, float(ms[0])
+
+    def info(self):
+        """(graph captures so far, slot capacities [n], pool capacities in points [n])."""
+        cap = C.c_int()
+        sl = np.zeros(self.n, dtype=np.int32)
+        pool = np.zeros(self.n, dtype=np.int64)
+        check(self.lib.csl_multi_info(self.p, C.byref(cap), iptr(sl),
+                                      pool.ctypes.data_as(C.POINTER(C.c_longlong))))
+        return cap.value, sl, pool
+
+    def close(self):
+        if getattr(self, "p", None):
+            self.lib.csl_multi_destroy(self.p)
+            self.p = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

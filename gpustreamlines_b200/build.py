@@ -15,7 +15,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "_csl.so")
-SOURCES = ["kernels.cu", "boot_batch.cu", "odf_gemm.cu", "compress.cu", "mlp.cu", "dti.cu", "capi.cu", "noalloc.cu"]
+SOURCES = ["kernels.cu", "boot_batch.cu", "odf_gemm.cu", "compress.cu", "mlp.cu", "dti.cu", "multi.cu", "capi.cu", "noalloc.cu"]
 NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "--use_fast_math", "-lineinfo",
               "-std=c++17", "-Xcompiler", "-fPIC", "-shared", "-diag-suppress", "20281"]
 

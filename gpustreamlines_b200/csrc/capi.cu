@@ -698,6 +698,7 @@ static int run_batch(csl_tracker *t, const float *seeds_dev, long long n, long l
         B.pool_cap = t->pool.cap / 3;
         B.scratch = t->scratch.p;
         B.status = t->status.p;
+        B.sl_cap = nsl;
         if (t->hp.seed_order == 1) {
             size_t sb = t->sort_tmp.cap;
             CK(spatial_order(seeds_dev, ni, grid2, t->mkeys.p, t->mkeys_sorted.p, t->mvals.p, t->perm.p,
@@ -1020,6 +1021,460 @@ int csl_philox_stream(unsigned long long seed, unsigned long long subsequence,
     d.release();
     CK(e);
     return CSL_OK;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Multi-subject run: the batches of many trackers (subjects) as independent
+// branches of ONE captured CUDA graph, launched with one cudaGraphLaunch.
+//
+// Each branch is the plain batch path without its host round trips: pass 1
+// (seed peaks) and its scan, pass 2 (the persistent tracking kernel) into a
+// point pool and streamline slots of fixed capacity, then the device-counted
+// scan and gather of multi.cu, and a four-value summary.  Branches share no
+// buffer, so the GPU runs their CTAs side by side: the tail of one subject's
+// persistent kernel is filled by the next subject's CTAs.  Capacities come
+// from a pass-1 count at plan creation (slots) and a points-per-streamline
+// estimate (pool); a subject that overflows either is re-run on the plain
+// path by csl_multi_wait (exact sizes, same streamlines) and its capacities
+// grow for the next capture.  Before every launch the plan compares the
+// device buffers and launch shape each branch was captured with against the
+// trackers' current ones and re-captures when any changed.
+
+struct csl_multi {
+    int device = 0;
+    int nsub = 0;
+    std::vector<csl_tracker *> sub;
+    std::vector<const float *> seeds;
+    std::vector<long long> n, rng_base;
+    std::vector<int> sl_cap;
+    std::vector<unsigned long long> pool_cap;  // points
+    std::vector<std::vector<const void *>> captured;
+    std::vector<DevBuf<unsigned char>> scan_tmp;
+    std::vector<DevBuf<long long>> bsum;
+    DevBuf<long long> summary;  // [nsub][4]: streamlines, points, status, pool points used
+    long long *summary_h = nullptr;
+    cudaStream_t st = nullptr, launch_st = nullptr;
+    std::vector<cudaStream_t> br;
+    std::vector<cudaEvent_t> join;
+    cudaEvent_t fork = nullptr, ev0 = nullptr, ev1 = nullptr;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    bool dirty = true, in_flight = false;
+    int captures = 0;
+    float ms = 0;
+};
+
+static std::vector<const void *> branch_fingerprint(const csl_tracker *u) {
+    return {u->npeaks.p, u->sl_off.p, u->peaks.p, u->out_len.p, u->out_seed.p, u->out_src.p, u->pt_off.p,
+            u->pool.p, u->points.p, u->scratch.p, u->queue.p, u->status.p, u->pool_count.p, u->sort_tmp.p,
+            u->mkeys.p, u->mkeys_sorted.p, u->mvals.p, u->perm.p, u->blk_next.p, u->blk_end.p,
+            (const void *)(intptr_t)u->block, (const void *)(intptr_t)u->blocks_per_sm,
+            (const void *)(intptr_t)u->hp.seed_order};
+}
+
+static int branch_grid(const csl_tracker *u, long long ni) {
+    const int wpb = u->block / kWarp;
+    return (int)std::max<long long>(1, std::min<long long>((long long)u->nsm * u->blocks_per_sm, (ni + wpb - 1) / wpb));
+}
+
+// grow subject i's buffers to the plan's capacities (no-op when they fit)
+static int multi_size(csl_multi *m, int i) {
+    csl_tracker *t = nullptr;  // errors go to the library-wide message
+    csl_tracker *u = m->sub[i];
+    const long long ni = m->n[i];
+    const int cap = m->sl_cap[i];
+    const unsigned long long pc = m->pool_cap[i];
+    CK(u->npeaks.ensure(ni + 1));
+    CK(u->sl_off.ensure(ni + 1));
+    CK(u->peaks.ensure((size_t)ni * kMaxStoredPeaksPerSeed));
+    size_t tb = 0;
+    CK(scan_temp_bytes((int)ni + 1, &tb));
+    CK(m->scan_tmp[i].ensure(tb));
+    CK(m->bsum[i].ensure(kCountedScanBlocks));
+    CK(u->out_len.ensure((size_t)cap + 1));
+    CK(u->out_seed.ensure((size_t)cap + 1));
+    CK(u->out_src.ensure((size_t)cap + 1));
+    CK(u->pt_off.ensure((size_t)cap + 1));
+    CK(u->pool.ensure((size_t)pc * 3));
+    CK(u->points.ensure((size_t)pc * 3 + 3));
+    const int grid2 = branch_grid(u, ni);
+    CK(u->scratch.ensure((size_t)grid2 * (u->block / kWarp) * scratch_floats_per_warp(u->P)));
+    if (u->hp.seed_order == 1) {
+        size_t sb = 0;
+        CK(spatial_order(nullptr, (int)ni, grid2, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr,
+                         &sb, 0));
+        CK(u->sort_tmp.ensure(sb));
+        CK(u->mkeys.ensure(ni));
+        CK(u->mkeys_sorted.ensure(ni));
+        CK(u->mvals.ensure(ni));
+        CK(u->perm.ensure(ni));
+        CK(u->blk_next.ensure(grid2));
+        CK(u->blk_end.ensure(grid2));
+    }
+    return CSL_OK;
+}
+
+// record subject i's batch on stream s (inside the capture)
+static int multi_record(csl_multi *m, int i, cudaStream_t s) {
+    csl_tracker *t = nullptr;
+    csl_tracker *u = m->sub[i];
+    const DevParams &P = u->P;
+    const int ni = (int)m->n[i];
+    const int cap = m->sl_cap[i];
+    const int wpb = u->block / kWarp;
+    const int grid1 = (int)std::min<long long>(((long long)ni + wpb - 1) / wpb, (long long)u->nsm * 16);
+    const int grid2 = branch_grid(u, ni);
+    CK(cudaMemsetAsync(u->npeaks.p + ni, 0, sizeof(int), s));
+    CK(launch_seed_peaks(P, m->seeds[i], ni, m->rng_base[i], u->partner.p, u->npeaks.p, u->peaks.p,
+                         kMaxStoredPeaksPerSeed, grid1, u->block, s));
+    CK(exclusive_scan_i32(m->scan_tmp[i].p, m->scan_tmp[i].cap, u->npeaks.p, u->sl_off.p, ni + 1, s));
+    BatchArgs B{};
+    B.seeds = m->seeds[i];
+    B.nseeds = ni;
+    B.rng_index_base = m->rng_base[i];
+    B.queue = u->queue.p;
+    B.pool_count = u->pool_count.p;
+    B.pool = u->pool.p;
+    B.pool_cap = m->pool_cap[i];
+    B.scratch = u->scratch.p;
+    B.status = u->status.p;
+    B.sl_cap = cap;
+    if (u->hp.seed_order == 1) {
+        size_t sb = u->sort_tmp.cap;
+        CK(spatial_order(m->seeds[i], ni, grid2, u->mkeys.p, u->mkeys_sorted.p, u->mvals.p, u->perm.p,
+                         u->blk_next.p, u->blk_end.p, u->sort_tmp.p, &sb, s));
+        B.perm = u->perm.p;
+        B.blk_next = u->blk_next.p;
+        B.blk_end = u->blk_end.p;
+    }
+    CK(cudaMemsetAsync(u->queue.p, 0, sizeof(int), s));
+    CK(cudaMemsetAsync(u->status.p, 0, sizeof(int), s));
+    CK(cudaMemsetAsync(u->pool_count.p, 0, sizeof(unsigned long long), s));
+    CK(launch_track(P, B, u->partner.p, u->npeaks.p, u->peaks.p, kMaxStoredPeaksPerSeed, u->sl_off.p,
+                    u->out_len.p, u->out_seed.p, u->out_src.p, grid2, u->block, s));
+    const int *count = u->sl_off.p + ni;
+    CK(launch_counted_scan(u->out_len.p, count, cap, m->bsum[i].p, u->pt_off.p, s));
+    CK(launch_gather_counted(u->pool.p, u->out_src.p, u->out_len.p, u->pt_off.p, count, cap, u->status.p,
+                             (long long)m->pool_cap[i], u->points.p, u->nsm * 8, s));
+    CK(launch_batch_summary(count, cap, u->pt_off.p, u->status.p, u->pool_count.p, m->summary.p + 4 * i, s));
+    return CSL_OK;
+}
+
+static int multi_capture(csl_multi *m) {
+    csl_tracker *t = nullptr;
+    if (m->exec) cudaGraphExecDestroy(m->exec);
+    if (m->graph) cudaGraphDestroy(m->graph);
+    m->exec = nullptr;
+    m->graph = nullptr;
+    CK(cudaStreamBeginCapture(m->st, cudaStreamCaptureModeRelaxed));
+    int rc = CSL_OK;
+    cudaError_t e = cudaEventRecord(m->fork, m->st);
+    for (int i = 0; i < m->nsub && rc == CSL_OK && e == cudaSuccess; i++) {
+        if (m->n[i] == 0) continue;
+        e = cudaStreamWaitEvent(m->br[i], m->fork, 0);
+        if (e == cudaSuccess) rc = multi_record(m, i, m->br[i]);
+        if (rc == CSL_OK && e == cudaSuccess) e = cudaEventRecord(m->join[i], m->br[i]);
+        if (rc == CSL_OK && e == cudaSuccess) e = cudaStreamWaitEvent(m->st, m->join[i], 0);
+    }
+    if (rc == CSL_OK && e == cudaSuccess)
+        e = cudaMemcpyAsync(m->summary_h, m->summary.p, (size_t)m->nsub * 4 * sizeof(long long),
+                            cudaMemcpyDeviceToHost, m->st);
+    cudaGraph_t g = nullptr;
+    const cudaError_t e2 = cudaStreamEndCapture(m->st, &g);
+    if (rc != CSL_OK || e != cudaSuccess || e2 != cudaSuccess) {
+        if (g) cudaGraphDestroy(g);
+        if (rc != CSL_OK) return rc;
+        CK(e != cudaSuccess ? e : e2);
+    }
+    m->graph = g;
+    CK(cudaGraphInstantiate(&m->exec, g, 0));
+    m->captures++;
+    for (int i = 0; i < m->nsub; i++) m->captured[i] = branch_fingerprint(m->sub[i]);
+    m->dirty = false;
+    return CSL_OK;
+}
+
+static void multi_release(csl_multi *m) {
+    if (m->exec) cudaGraphExecDestroy(m->exec);
+    if (m->graph) cudaGraphDestroy(m->graph);
+    for (auto &b : m->scan_tmp) b.release();
+    for (auto &b : m->bsum) b.release();
+    m->summary.release();
+    if (m->summary_h) cudaFreeHost(m->summary_h);
+    for (auto s : m->br)
+        if (s) cudaStreamDestroy(s);
+    for (auto ev : m->join)
+        if (ev) cudaEventDestroy(ev);
+    cudaEvent_t evs[] = {m->fork, m->ev0, m->ev1};
+    for (auto ev : evs)
+        if (ev) cudaEventDestroy(ev);
+    if (m->st) cudaStreamDestroy(m->st);
+}
+
+extern "C" {
+
+int csl_multi_create(csl_tracker *const *subjects, const float *const *seeds_dev, const long long *n_seeds,
+                     const long long *rng_index_base, int n_subjects, int points_per_streamline,
+                     csl_multi **out) {
+    csl_tracker *t = nullptr;
+    if (!out) return fail(nullptr, CSL_E_INVALID, "NULL output");
+    *out = nullptr;
+    if (n_subjects < 1 || !subjects || !seeds_dev || !n_seeds)
+        return fail(nullptr, CSL_E_INVALID, "csl_multi_create: need at least one subject");
+    if (points_per_streamline < 0) return fail(nullptr, CSL_E_INVALID, "points_per_streamline must be >= 0");
+    for (int i = 0; i < n_subjects; i++) {
+        if (!subjects[i]) return fail(nullptr, CSL_E_INVALID, "subject %d is NULL", i);
+        if (subjects[i]->device != subjects[0]->device)
+            return fail(nullptr, CSL_E_INVALID, "all subjects must be on one device");
+        if (n_seeds[i] < 0 || n_seeds[i] > (1ll << 30) || (n_seeds[i] > 0 && !seeds_dev[i]))
+            return fail(nullptr, CSL_E_INVALID, "subject %d: bad seeds", i);
+        for (int j = 0; j < i; j++)
+            if (subjects[j] == subjects[i]) return fail(nullptr, CSL_E_INVALID, "subject %d repeats subject %d", i, j);
+    }
+    csl_multi *m = new csl_multi();
+    m->nsub = n_subjects;
+    m->device = subjects[0]->device;
+    m->sub.assign(subjects, subjects + n_subjects);
+    m->seeds.assign(seeds_dev, seeds_dev + n_subjects);
+    m->n.assign(n_seeds, n_seeds + n_subjects);
+    m->rng_base.assign(n_subjects, 0);
+    if (rng_index_base)
+        for (int i = 0; i < n_subjects; i++) m->rng_base[i] = rng_index_base[i];
+    m->sl_cap.assign(n_subjects, 0);
+    m->pool_cap.assign(n_subjects, 0);
+    m->captured.resize(n_subjects);
+    m->scan_tmp.resize(n_subjects);
+    m->bsum.resize(n_subjects);
+    m->br.assign(n_subjects, nullptr);
+    m->join.assign(n_subjects, nullptr);
+    auto bail = [&](int rc) {
+        multi_release(m);
+        delete m;
+        return rc;
+    };
+#define MK(call)                                                                                   \
+    do {                                                                                           \
+        cudaError_t _e = (call);                                                                   \
+        if (_e != cudaSuccess)                                                                     \
+            return bail(fail(nullptr, _e == cudaErrorMemoryAllocation ? CSL_E_NOMEM : CSL_E_CUDA, \
+                             "CUDA error code=%d(%s) at %s:%d", (int)_e, cudaGetErrorName(_e),     \
+                             __FILE__, __LINE__));                                                 \
+    } while (0)
+    MK(cudaSetDevice(m->device));
+    MK(cudaStreamCreateWithFlags(&m->st, cudaStreamNonBlocking));
+    for (int i = 0; i < n_subjects; i++) {
+        MK(cudaStreamCreateWithFlags(&m->br[i], cudaStreamNonBlocking));
+        MK(cudaEventCreateWithFlags(&m->join[i], cudaEventDisableTiming));
+    }
+    MK(cudaEventCreateWithFlags(&m->fork, cudaEventDisableTiming));
+    MK(cudaEventCreate(&m->ev0));
+    MK(cudaEventCreate(&m->ev1));
+    MK(m->summary.ensure((size_t)n_subjects * 4));
+    MK(cudaMemset(m->summary.p, 0, (size_t)n_subjects * 4 * sizeof(long long)));
+    MK(cudaMallocHost(&m->summary_h, (size_t)n_subjects * 4 * sizeof(long long)));
+    // slot capacity from a pass-1 count of each subject's seeds (plus margin
+    // for seeds rewritten in place before a later launch)
+    const long long ppsl = points_per_streamline > 0 ? points_per_streamline : 128;
+    for (int i = 0; i < n_subjects; i++) {
+        csl_tracker *u = m->sub[i];
+        const long long ni = m->n[i];
+        long long nsl = 0;
+        if (ni > 0) {
+            MK(u->npeaks.ensure(ni + 1));
+            MK(u->sl_off.ensure(ni + 1));
+            MK(u->peaks.ensure((size_t)ni * kMaxStoredPeaksPerSeed));
+            size_t tb = 0;
+            MK(scan_temp_bytes((int)ni + 1, &tb));
+            MK(u->scan_tmp.ensure(tb));
+            const int wpb = u->block / kWarp;
+            const int grid1 = (int)std::min<long long>((ni + wpb - 1) / wpb, (long long)u->nsm * 16);
+            MK(cudaMemsetAsync(u->npeaks.p + ni, 0, sizeof(int), m->st));
+            MK(launch_seed_peaks(u->P, m->seeds[i], (int)ni, m->rng_base[i], u->partner.p, u->npeaks.p,
+                                 u->peaks.p, kMaxStoredPeaksPerSeed, grid1, u->block, m->st));
+            MK(exclusive_scan_i32(u->scan_tmp.p, u->scan_tmp.cap, u->npeaks.p, u->sl_off.p, (int)ni + 1, m->st));
+            int c = 0;
+            MK(cudaMemcpyAsync(&c, u->sl_off.p + ni, sizeof(int), cudaMemcpyDeviceToHost, m->st));
+            MK(cudaStreamSynchronize(m->st));
+            nsl = c;
+        }
+        const long long cap = std::min<long long>(nsl + nsl / 16 + 256, (long long)INT32_MAX - 1);
+        m->sl_cap[i] = (int)cap;
+        m->pool_cap[i] = (unsigned long long)(cap * ppsl);
+    }
+#undef MK
+    *out = m;
+    return CSL_OK;
+}
+
+int csl_multi_launch(csl_multi *m, void *stream) {
+    csl_tracker *t = nullptr;
+    if (!m) return fail(nullptr, CSL_E_INVALID, "NULL plan");
+    if (m->in_flight) return fail(nullptr, CSL_E_STATE, "csl_multi_launch: wait for the previous launch first");
+    CK(cudaSetDevice(m->device));
+    for (int i = 0; i < m->nsub; i++) {
+        if (m->n[i] == 0) continue;
+        const int rc = multi_size(m, i);
+        if (rc != CSL_OK) return rc;
+        if (m->captured[i] != branch_fingerprint(m->sub[i])) m->dirty = true;
+    }
+    if (m->dirty) {
+        const int rc = multi_capture(m);
+        if (rc != CSL_OK) return rc;
+    }
+    m->launch_st = stream ? (cudaStream_t)stream : m->st;
+    CK(cudaEventRecord(m->ev0, m->launch_st));
+    CK(cudaGraphLaunch(m->exec, m->launch_st));
+    CK(cudaEventRecord(m->ev1, m->launch_st));
+    m->in_flight = true;
+    return CSL_OK;
+}
+
+int csl_multi_wait(csl_multi *m, long long *n_streamlines, long long *n_points, int *replayed, float *ms) {
+    csl_tracker *t = nullptr;
+    if (!m) return fail(nullptr, CSL_E_INVALID, "NULL plan");
+    if (!m->in_flight) return fail(nullptr, CSL_E_STATE, "csl_multi_wait: nothing launched");
+    CK(cudaSetDevice(m->device));
+    CK(cudaStreamSynchronize(m->launch_st));
+    m->in_flight = false;
+    CK(cudaEventElapsedTime(&m->ms, m->ev0, m->ev1));
+    if (ms) *ms = m->ms;
+    for (int i = 0; i < m->nsub; i++) {
+        csl_tracker *u = m->sub[i];
+        const long long *S = m->summary_h + 4 * i;
+        int again = 0;
+        if (m->n[i] > 0 && (S[2] & (ST_POOL_OVERFLOW | ST_SLOT_OVERFLOW))) {
+            const int rc = run_batch(u, m->seeds[i], m->n[i], m->rng_base[i], u->own_stream);
+            if (rc != CSL_OK) return fail(nullptr, rc, "subject %d: %s", i, u->err.c_str());
+            m->sl_cap[i] = (int)std::min<long long>(
+                std::max<long long>(m->sl_cap[i], u->nsl + u->nsl / 8 + 256), (long long)INT32_MAX - 1);
+            m->pool_cap[i] = std::max<unsigned long long>(m->pool_cap[i],
+                                                          (unsigned long long)(u->npts + u->npts / 8 + 4096));
+            m->dirty = true;
+            again = 1;
+        } else if (m->n[i] > 0 && S[2] != 0) {
+            return fail(nullptr, CSL_E_KERNEL, "subject %d: kernel status %lld", i, S[2]);
+        } else {
+            u->ok_batch = 1;
+            u->cmp_npts = -1;
+            u->last_n = m->n[i];
+            u->last_stream = m->launch_st;
+            u->nsl = m->n[i] > 0 ? S[0] : 0;
+            u->npts = m->n[i] > 0 ? S[1] : 0;
+            u->pass2_runs = 1;
+            for (float &x : u->ms) x = 0;
+        }
+        if (n_streamlines) n_streamlines[i] = u->nsl;
+        if (n_points) n_points[i] = u->npts;
+        if (replayed) replayed[i] = again;
+    }
+    return CSL_OK;
+}
+
+int csl_multi_info(csl_multi *m, int *captures, int *slot_caps, long long *pool_caps) {
+    if (!m) return fail(nullptr, CSL_E_INVALID, "NULL plan");
+    if (captures) *captures = m->captures;
+    for (int i = 0; i < m->nsub; i++) {
+        if (slot_caps) slot_caps[i] = m->sl_cap[i];
+        if (pool_caps) pool_caps[i] = (long long)m->pool_cap[i];
+    }
+    return CSL_OK;
+}
+
+int csl_multi_destroy(csl_multi *m) {
+    if (!m) return CSL_OK;
+    cudaSetDevice(m->device);
+    if (m->in_flight) cudaStreamSynchronize(m->launch_st);
+    multi_release(m);
+    delete m;
+    return CSL_OK;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Launch-shape tuning of the per-warp tracking path: threads per CTA of the
+// pass-1 and pass-2 kernels (64, 128 or 256; CTAs per SM follow from the
+// occupancy calculator) and the seed schedule (input or Morton order).
+// Neither changes a streamline -- the RNG stream of a seed depends only on
+// the seed's index -- so the tuner only times them.
+
+// the tracking kernel's shared memory at this CTA size stays within the
+// per-CTA limit (asked of the occupancy calculator only then)
+static bool launch_fits(const csl_tracker *t, int block) {
+    return smem_bytes(t->P, block / kWarp, true) <= 227 * 1024;
+}
+
+static int set_launch(csl_tracker *t, int block, int seed_order) {
+    if (block != 64 && block != 128 && block != 256)
+        return fail(t, CSL_E_INVALID, "threads per CTA must be 64, 128 or 256");
+    if (seed_order != 0 && seed_order != 1) return fail(t, CSL_E_INVALID, "seed_order must be 0 or 1");
+    if (!launch_fits(t, block))
+        return fail(t, CSL_E_INVALID, "%d threads per CTA do not fit on the device", block);
+    int bps = 0;
+    CK(track_occupancy(t->P, block, &bps));
+    if (bps < 1) return fail(t, CSL_E_INVALID, "%d threads per CTA do not fit on the device", block);
+    t->block = block;
+    t->blocks_per_sm = bps;
+    t->hp.seed_order = seed_order;
+    return CSL_OK;
+}
+
+extern "C" {
+
+int csl_set_launch(csl_tracker *t, int threads_per_block, int seed_order) {
+    if (!t) return fail(nullptr, CSL_E_INVALID, "NULL tracker");
+    CK(cudaSetDevice(t->device));
+    return set_launch(t, threads_per_block, seed_order);
+}
+
+int csl_get_launch(csl_tracker *t, int *threads_per_block, int *seed_order, int *blocks_per_sm) {
+    if (!t) return fail(nullptr, CSL_E_INVALID, "NULL tracker");
+    if (threads_per_block) *threads_per_block = t->block;
+    if (seed_order) *seed_order = t->hp.seed_order;
+    if (blocks_per_sm) *blocks_per_sm = t->blocks_per_sm;
+    return CSL_OK;
+}
+
+int csl_autotune(csl_tracker *t, const float *seeds_dev, long long n, long long rng_index_base, int repeats,
+                 float *ms_out) {
+    if (!t) return fail(nullptr, CSL_E_INVALID, "NULL tracker");
+    if (n < 1 || !seeds_dev) return fail(t, CSL_E_INVALID, "csl_autotune: need a seed sample");
+    if (repeats < 1) return fail(t, CSL_E_INVALID, "csl_autotune: repeats must be >= 1");
+    CK(cudaSetDevice(t->device));
+    static const int kBlocks[3] = {256, 128, 64};
+    const int block0 = t->block, order0 = t->hp.seed_order;
+    float best = -1.0f;
+    int best_b = block0, best_o = order0;
+    for (int c = 0; c < 6; c++) {
+        const int b = kBlocks[c / 2], o = c % 2;
+        float total = -1.0f;
+        int bps = 0;
+        if (launch_fits(t, b)) CK(track_occupancy(t->P, b, &bps));
+        if (bps >= 1) {
+            t->block = b;
+            t->blocks_per_sm = bps;
+            t->hp.seed_order = o;
+            int rc = run_batch(t, seeds_dev, n, rng_index_base, t->own_stream);  // warm-up, sizes buffers
+            for (int r = 0; r < repeats && rc == CSL_OK; r++) {
+                rc = run_batch(t, seeds_dev, n, rng_index_base, t->own_stream);
+                const float ms = t->ms[0] + t->ms[1] + t->ms[2] + t->ms[3];
+                if (total < 0 || ms < total) total = ms;
+            }
+            if (rc != CSL_OK) {
+                set_launch(t, block0, order0);
+                return rc;
+            }
+            if (best < 0 || total < best) {
+                best = total;
+                best_b = b;
+                best_o = o;
+            }
+        }
+        if (ms_out) ms_out[c] = total;
+    }
+    return set_launch(t, best_b, best_o);
 }
 
 }  // extern "C"

@@ -76,12 +76,15 @@ struct BatchArgs {
     unsigned long long pool_cap;
     float *scratch;                     // per-warp point buffers + peak list
     int *status;                        // error/overflow flags
+    int sl_cap;                         // streamline slots in out_len / out_seed / out_src: a seed
+                                        // whose slots would pass it is skipped and flagged
 };
 
 enum StatusBits {
     ST_POOL_OVERFLOW = 1,   // point pool too small: the batch is re-run with an exact size
     ST_PEAKS_OVERFLOW = 2,  // a seed has more initial directions than pass 1 stores
     ST_WAIT_TIMEOUT = 4,    // a bounded wait on an mbarrier gave up (never expected)
+    ST_SLOT_OVERFLOW = 8,   // more streamlines than the fixed slot capacity of a graph-captured batch
 };
 
 // ---------------------------------------------------------------------------

@@ -138,6 +138,11 @@ __global__ void __launch_bounds__(256, MODEL == PROB ? CSL_PROB_MIN_BLOCKS
         if (s >= B.nseeds) break;
         const int np = npeaks[s];
         if (np == 0) continue;
+        const int base = sl_off[s];
+        if (base + np > B.sl_cap) {
+            if (lane == 0) atomicOr(B.status, ST_SLOT_OVERFLOW);
+            continue;
+        }
         const float3 seed = make_float3(B.seeds[3 * s], B.seeds[3 * s + 1], B.seeds[3 * s + 2]);
         const unsigned long long gid = 32ull * (unsigned long long)(s + B.rng_index_base) + lane;
         // peak list: stored by pass 1, or recomputed into this warp's scratch
@@ -151,7 +156,6 @@ __global__ void __launch_bounds__(256, MODEL == PROB ? CSL_PROB_MIN_BLOCKS
         typename RngOf<MODEL>::T rng;
         if constexpr (MODEL == PROB) rng.st = W.rng;
         rng.init(P.rng_seed, gid + 1, 0);
-        const int base = sl_off[s];
         {
             for (int k = 0; k < np; k++) {
                 const int pv = (np > max_store) ? plist[k] : (int)stored[k];

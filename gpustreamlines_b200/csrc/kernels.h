@@ -106,6 +106,16 @@ cudaError_t launch_compress_gather(const float *world, const long long *off, con
                                    const unsigned char *keep, const long long *coff, int nsl, float *out,
                                    cudaStream_t st);
 
+// ---- device-counted compaction for graph-captured batches (multi.cu)
+constexpr int kCountedScanBlocks = 1024;  // CTAs of the counted scan = length of its partial-sum buffer
+cudaError_t launch_counted_scan(const int *len, const int *count, int cap, long long *bsum, long long *pt_off,
+                                cudaStream_t st);
+cudaError_t launch_gather_counted(const float *pool, const long long *src, const int *len, const long long *pt_off,
+                                  const int *count, int cap, const int *status, long long pts_cap, float *out,
+                                  int grid, cudaStream_t st);
+cudaError_t launch_batch_summary(const int *count, int cap, const long long *pt_off, const int *status,
+                                 const unsigned long long *pool_count, long long *out4, cudaStream_t st);
+
 cudaError_t scan_temp_bytes(int n, size_t *bytes);
 // Morton-sort the seeds (perm = position -> seed) and split the order into
 // per-block ranges; with tmp == nullptr only reports the sort's temp size.

@@ -300,6 +300,58 @@ int csl_dti_fa(const float *dwi_dev, long long nvox, int T, const double *bvals,
 int csl_seeds_from_mask(const float *mask_dev, int X, int Y, int Z, float threshold, long long n,
                         unsigned long long seed, float *seeds_dev, long long *nvox_out, void *stream);
 
+/*
+ * Multi-subject run (no counterpart in the reference, which tracks one
+ * subject per GPUTracker and per call; replaces a host loop of
+ * GPUTracker.generate_streamlines / _propagate calls, cu_tractography.py:264-300).
+ * A plan binds n_subjects trackers (one device, each tracker at most once)
+ * to their seed batches (device float32 [n_seeds[i], 3]; pointers and counts
+ * fixed for the plan's life, contents may be rewritten between launches) and
+ * runs every batch as one branch of ONE captured CUDA graph: per subject,
+ * pass 1, pass 2 (the per-warp tracking path; boot_fit = 1 trackers use it
+ * too) and compaction into the tracker's own result buffers, with no host
+ * round trip.  Streamlines are identical to csl_propagate_device's on each
+ * tracker.  Slot capacity comes from a pass-1 count at creation, pool
+ * capacity from points_per_streamline (0: 128); a subject that overflows
+ * either is re-run on the plain path inside csl_multi_wait (replayed[i] = 1)
+ * and its capacities grow for the next launch, which re-captures the graph
+ * (it also re-captures when a tracker's buffers or launch shape changed).
+ *   csl_multi_launch  one cudaGraphLaunch on stream (NULL: the plan's own)
+ *   csl_multi_wait    waits, finishes overflowed subjects; per subject
+ *                     n_streamlines / n_points (arrays of n_subjects, may be
+ *                     NULL); *ms = device time of the graph launch.  Results
+ *                     are then read per tracker: csl_counts, csl_fetch,
+ *                     csl_device_results, csl_compress.
+ *   csl_multi_info    graph captures so far, slot / pool capacities
+ * Destroy the plan before its trackers.  Errors: csl_last_error(NULL, ...).
+ */
+typedef struct csl_multi csl_multi;
+int csl_multi_create(csl_tracker *const *subjects, const float *const *seeds_dev, const long long *n_seeds,
+                     const long long *rng_index_base, int n_subjects, int points_per_streamline,
+                     csl_multi **out);
+int csl_multi_launch(csl_multi *plan, void *stream);
+int csl_multi_wait(csl_multi *plan, long long *n_streamlines, long long *n_points, int *replayed, float *ms);
+int csl_multi_info(csl_multi *plan, int *captures, int *slot_caps, long long *pool_caps);
+int csl_multi_destroy(csl_multi *plan);
+
+/*
+ * Launch shape of the per-warp tracking path (no counterpart in the
+ * reference, which fixes 128 threads per block and one CTA grid per call,
+ * cu_tractography.py:275-300).  threads_per_block 64, 128 or 256 (CTAs per SM
+ * from the occupancy calculator), seed_order 0 (input order) or 1 (Morton
+ * order).  Streamlines do not depend on either.
+ *   csl_autotune  times the 6 shapes on a device seed sample (one warm-up
+ *                 plus `repeats` batches each, best of the repeats: pass 1,
+ *                 pass 2 and compaction), keeps the fastest; ms_out[6]
+ *                 (optional) = the times in the order (256,0) (256,1)
+ *                 (128,0) (128,1) (64,0) (64,1), -1 for a shape that does
+ *                 not fit.  The tracker's last batch is then the sample's.
+ */
+int csl_set_launch(csl_tracker *t, int threads_per_block, int seed_order);
+int csl_get_launch(csl_tracker *t, int *threads_per_block, int *seed_order, int *blocks_per_sm);
+int csl_autotune(csl_tracker *t, const float *seeds_dev, long long n, long long rng_index_base, int repeats,
+                 float *ms_out);
+
 const char *csl_version(void);
 
 #ifdef __cplusplus

@@ -92,6 +92,15 @@ def test_library_rejects_bad_arguments_without_gpu():
     assert rc == _lib.CSL_E_INVALID
     assert "NULL" in _lib.last_error()
     assert lib.csl_counts(None, None, None) == _lib.CSL_E_INVALID
+    # multi-subject plan and launch-shape calls validate before touching a device
+    plan = C.c_void_p()
+    assert lib.csl_multi_create(None, None, None, None, 0, 0, C.byref(plan)) == _lib.CSL_E_INVALID
+    assert "subject" in _lib.last_error()
+    assert lib.csl_multi_launch(None, None) == _lib.CSL_E_INVALID
+    assert lib.csl_multi_wait(None, None, None, None, None) == _lib.CSL_E_INVALID
+    assert lib.csl_multi_destroy(None) == _lib.CSL_OK
+    assert lib.csl_set_launch(None, 128, 0) == _lib.CSL_E_INVALID
+    assert lib.csl_autotune(None, None, 0, 0, 1, None) == _lib.CSL_E_INVALID
 
 
 def test_tracker_validation_matches_reference_errors():
