@@ -306,8 +306,9 @@ def multi_subjects(nsub: int, seed: int = 5):
     """Uneven synthetic subjects for the multi-subject run: volumes log-uniform
     between 48^3 and 96x116x96 voxels (phantom shape scaled), two diffusion
     schemes (6 b0 + 64 dirs at b=1000, 2.5 mm; 10 b0 + 150 dirs at b=2000,
-    2 mm), seeds log-uniform in [5k, 250k] (a fifth of that for bootstrap
-    and PTT subjects, whose steps cost 15-50x a probabilistic step), getters
+    2 mm), seeds log-uniform in [5k, 250k] (1/25 of that, at least 1000,
+    for bootstrap and PTT subjects, whose steps cost 40-120x a probabilistic
+    step), getters
     cycling probabilistic, bootstrap CSA, PTT, probabilistic, bootstrap OPDT,
     probabilistic."""
     rng = np.random.default_rng(seed)
@@ -320,7 +321,7 @@ def multi_subjects(nsub: int, seed: int = 5):
         shape = tuple(max(24, int(round(d * scale))) for d in (81, 106, 76))
         n_b0, n_dirs, bval, mm = [(6, 64, 1000.0, 2.5), (10, 150, 2000.0, 2.0)][i % 2]
         getter = cycle[i % len(cycle)]
-        n = int(nseeds[i]) if getter == "prob" else max(1000, int(nseeds[i]) // 5)
+        n = int(nseeds[i]) if getter == "prob" else max(1000, int(nseeds[i]) // 25)
         out.append(dict(getter=getter, shape=shape, n_b0=n_b0, n_dirs=n_dirs, bval=bval,
                         voxel_mm=mm, seeds=n, seed=100 + i))
     return out
@@ -364,9 +365,13 @@ def run_multi(args):
     nsl, npts, rep, _ = run.last
     steps = int((npts - nsl).sum())
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    replays, graph_ms = 0, []
-    torch.cuda.synchronize()
-    with ClockSampler(0) as clk:
+
+    def timed_graph(k):
+        run.plan.set_concurrency(k)
+        run.launch(stream.cuda_stream)  # re-capture, untimed
+        run.wait()
+        replays, graph_ms = 0, []
+        torch.cuda.synchronize()
         ev0.record(stream)
         for _ in range(args.steps):
             run.launch(stream.cuda_stream)
@@ -375,7 +380,14 @@ def run_multi(args):
             graph_ms.append(ms)
         ev1.record(stream)
         torch.cuda.synchronize()
-    multi_ms = ev0.elapsed_time(ev1) / args.steps
+        return ev0.elapsed_time(ev1) / args.steps, replays, float(np.median(graph_ms))
+
+    by_k = {}
+    for k in (0, 2):
+        by_k[k] = timed_graph(k)
+    with ClockSampler(0) as clk:
+        by_k[1] = timed_graph(1)  # the default, the reported value
+    multi_ms, replays, graph_med = by_k[1]
     captures, _, _ = run.plan.info()
 
     # the same batches one after another through the plain path
@@ -429,8 +441,9 @@ def run_multi(args):
                    "seeds_total": int(sum(len(s) for s in seeds)), "streamlines_total": int(nsl.sum()),
                    "steps_total": steps, "volume_bytes_total": vol_bytes,
                    "l2": "inputs (volumes) larger than L2; no flush", "setup_s": t_setup,
-                   "graph_device_ms": float(np.median(graph_ms)), "graph_captures": captures,
-                   "replays_in_timed_region": replays,
+                   "graph_device_ms": graph_med, "graph_captures": captures,
+                   "replays_in_timed_region": replays, "max_concurrent_tracking_kernels": 1,
+                   "ms_per_step_by_max_concurrent": {str(k): v[0] for k, v in sorted(by_k.items())},
                    "bootstrap_fit": "per-warp FP32 (the graph path)"},
         "sequential_plain": {"value": seq_steps / (seq_ms / 1e3), "ms_per_step": seq_ms,
                              "note": "same batches, one csl_propagate_device per subject in turn"},

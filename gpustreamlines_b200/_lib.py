@@ -69,6 +69,7 @@ EXPORTS = (
     "csl_mlp_gemm", "csl_mlp_bias_act", "csl_mlp_act_bwd", "csl_mlp_colsum", "csl_mlp_vmf_nll",
     "csl_mlp_adam", "csl_mlp_param_count", "csl_mlp_infer", "csl_dti_fa", "csl_seeds_from_mask",
     "csl_multi_create", "csl_multi_launch", "csl_multi_wait", "csl_multi_info", "csl_multi_destroy",
+    "csl_multi_set_concurrency",
     "csl_set_launch", "csl_get_launch", "csl_autotune",
 )
 
@@ -125,6 +126,7 @@ def load(path: str | None = None):
     lib.csl_multi_wait.argtypes = [vp, llp, llp, _ip, _fp]
     lib.csl_multi_info.argtypes = [vp, _ip, _ip, llp]
     lib.csl_multi_destroy.argtypes = [vp]
+    lib.csl_multi_set_concurrency.argtypes = [vp, C.c_int]
     lib.csl_set_launch.argtypes = [vp, C.c_int, C.c_int]
     lib.csl_get_launch.argtypes = [vp, _ip, _ip, _ip]
     lib.csl_autotune.argtypes = [vp, vp, ll, ll, C.c_int, _fp]
@@ -361,6 +363,10 @@ class MultiPlan:
         check(self.lib.csl_multi_wait(self.p, nsl.ctypes.data_as(llp), npts.ctypes.data_as(llp), iptr(rep),
                                       fptr(ms)))
         return nsl, npts, rep, float(ms[0])
+
+    def set_concurrency(self, max_concurrent: int):
+        """At most this many tracking kernels in flight (0: no limit); next launch re-captures."""
+        check(self.lib.csl_multi_set_concurrency(self.p, int(max_concurrent)))
 
     def info(self):
         """(graph captures so far, slot capacities [n], pool capacities in points [n])."""

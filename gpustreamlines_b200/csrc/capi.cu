@@ -1061,6 +1061,9 @@ struct csl_multi {
     cudaEvent_t fork = nullptr, ev0 = nullptr, ev1 = nullptr;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
+    std::vector<cudaEvent_t> tracked;  // end of each branch's tracking kernel (concurrency limit)
+    std::vector<int> order;            // branch order: grouped by getter, larger batches first
+    int max_concurrent = 0;            // tracking kernels in flight at once (0: no limit)
     bool dirty = true, in_flight = false;
     int captures = 0;
     float ms = 0;
@@ -1116,8 +1119,9 @@ static int multi_size(csl_multi *m, int i) {
     return CSL_OK;
 }
 
-// record subject i's batch on stream s (inside the capture)
-static int multi_record(csl_multi *m, int i, cudaStream_t s) {
+// record subject i's batch on stream s (inside the capture); its tracking
+// kernel starts after the event wait_for (another branch's tracking kernel)
+static int multi_record(csl_multi *m, int i, cudaStream_t s, cudaEvent_t wait_for) {
     csl_tracker *t = nullptr;
     csl_tracker *u = m->sub[i];
     const DevParams &P = u->P;
@@ -1152,8 +1156,10 @@ static int multi_record(csl_multi *m, int i, cudaStream_t s) {
     CK(cudaMemsetAsync(u->queue.p, 0, sizeof(int), s));
     CK(cudaMemsetAsync(u->status.p, 0, sizeof(int), s));
     CK(cudaMemsetAsync(u->pool_count.p, 0, sizeof(unsigned long long), s));
+    if (wait_for) CK(cudaStreamWaitEvent(s, wait_for, 0));
     CK(launch_track(P, B, u->partner.p, u->npeaks.p, u->peaks.p, kMaxStoredPeaksPerSeed, u->sl_off.p,
                     u->out_len.p, u->out_seed.p, u->out_src.p, grid2, u->block, s));
+    CK(cudaEventRecord(m->tracked[i], s));
     const int *count = u->sl_off.p + ni;
     CK(launch_counted_scan(u->out_len.p, count, cap, m->bsum[i].p, u->pt_off.p, s));
     CK(launch_gather_counted(u->pool.p, u->out_src.p, u->out_len.p, u->pt_off.p, count, cap, u->status.p,
@@ -1171,10 +1177,15 @@ static int multi_capture(csl_multi *m) {
     CK(cudaStreamBeginCapture(m->st, cudaStreamCaptureModeRelaxed));
     int rc = CSL_OK;
     cudaError_t e = cudaEventRecord(m->fork, m->st);
-    for (int i = 0; i < m->nsub && rc == CSL_OK && e == cudaSuccess; i++) {
-        if (m->n[i] == 0) continue;
+    std::vector<int> live;  // branches in order
+    for (int i : m->order)
+        if (m->n[i] > 0) live.push_back(i);
+    for (size_t j = 0; j < live.size() && rc == CSL_OK && e == cudaSuccess; j++) {
+        const int i = live[j];
+        const int k = m->max_concurrent;
+        cudaEvent_t wait_for = (k > 0 && (int)j >= k) ? m->tracked[live[j - k]] : nullptr;
         e = cudaStreamWaitEvent(m->br[i], m->fork, 0);
-        if (e == cudaSuccess) rc = multi_record(m, i, m->br[i]);
+        if (e == cudaSuccess) rc = multi_record(m, i, m->br[i], wait_for);
         if (rc == CSL_OK && e == cudaSuccess) e = cudaEventRecord(m->join[i], m->br[i]);
         if (rc == CSL_OK && e == cudaSuccess) e = cudaStreamWaitEvent(m->st, m->join[i], 0);
     }
@@ -1206,6 +1217,8 @@ static void multi_release(csl_multi *m) {
     for (auto s : m->br)
         if (s) cudaStreamDestroy(s);
     for (auto ev : m->join)
+        if (ev) cudaEventDestroy(ev);
+    for (auto ev : m->tracked)
         if (ev) cudaEventDestroy(ev);
     cudaEvent_t evs[] = {m->fork, m->ev0, m->ev1};
     for (auto ev : evs)
@@ -1249,6 +1262,14 @@ int csl_multi_create(csl_tracker *const *subjects, const float *const *seeds_dev
     m->bsum.resize(n_subjects);
     m->br.assign(n_subjects, nullptr);
     m->join.assign(n_subjects, nullptr);
+    m->tracked.assign(n_subjects, nullptr);
+    m->max_concurrent = 1;
+    m->order.resize(n_subjects);
+    for (int i = 0; i < n_subjects; i++) m->order[i] = i;
+    std::stable_sort(m->order.begin(), m->order.end(), [&](int a, int b) {
+        if (subjects[a]->P.model != subjects[b]->P.model) return subjects[a]->P.model < subjects[b]->P.model;
+        return n_seeds[a] > n_seeds[b];
+    });
     auto bail = [&](int rc) {
         multi_release(m);
         delete m;
@@ -1267,6 +1288,7 @@ int csl_multi_create(csl_tracker *const *subjects, const float *const *seeds_dev
     for (int i = 0; i < n_subjects; i++) {
         MK(cudaStreamCreateWithFlags(&m->br[i], cudaStreamNonBlocking));
         MK(cudaEventCreateWithFlags(&m->join[i], cudaEventDisableTiming));
+        MK(cudaEventCreateWithFlags(&m->tracked[i], cudaEventDisableTiming));
     }
     MK(cudaEventCreateWithFlags(&m->fork, cudaEventDisableTiming));
     MK(cudaEventCreate(&m->ev0));
@@ -1369,6 +1391,15 @@ int csl_multi_wait(csl_multi *m, long long *n_streamlines, long long *n_points, 
         if (n_points) n_points[i] = u->npts;
         if (replayed) replayed[i] = again;
     }
+    return CSL_OK;
+}
+
+int csl_multi_set_concurrency(csl_multi *m, int max_concurrent) {
+    if (!m) return fail(nullptr, CSL_E_INVALID, "NULL plan");
+    if (max_concurrent < 0) return fail(nullptr, CSL_E_INVALID, "max_concurrent must be >= 0");
+    if (m->in_flight) return fail(nullptr, CSL_E_STATE, "csl_multi_set_concurrency: a launch is in flight");
+    if (max_concurrent != m->max_concurrent) m->dirty = true;
+    m->max_concurrent = max_concurrent;
     return CSL_OK;
 }
 

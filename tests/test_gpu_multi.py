@@ -98,6 +98,11 @@ def test_multi_subject_graph_matches_plain_batches():
             plan.launch()
             rep = _check(plan, handles, ref2)
             assert not rep.any()
+            # any limit on concurrent tracking kernels (0: none) gives the same batches
+            for k in (0, 2, 5):
+                plan.set_concurrency(k)
+                plan.launch()
+                _check(plan, handles, ref2)
         finally:
             plan.close()
     finally:
