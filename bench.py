@@ -383,11 +383,11 @@ def run_multi(args):
         return ev0.elapsed_time(ev1) / args.steps, replays, float(np.median(graph_ms))
 
     by_k = {}
-    for k in (0, 2):
+    for k in (0, 1, 3):
         by_k[k] = timed_graph(k)
     with ClockSampler(0) as clk:
-        by_k[1] = timed_graph(1)  # the default, the reported value
-    multi_ms, replays, graph_med = by_k[1]
+        by_k[2] = timed_graph(2)  # the library default, the reported value
+    multi_ms, replays, graph_med = by_k[2]
     captures, _, _ = run.plan.info()
 
     # the same batches one after another through the plain path
@@ -442,7 +442,7 @@ def run_multi(args):
                    "steps_total": steps, "volume_bytes_total": vol_bytes,
                    "l2": "inputs (volumes) larger than L2; no flush", "setup_s": t_setup,
                    "graph_device_ms": graph_med, "graph_captures": captures,
-                   "replays_in_timed_region": replays, "max_concurrent_tracking_kernels": 1,
+                   "replays_in_timed_region": replays, "max_concurrent_tracking_kernels": 2,
                    "ms_per_step_by_max_concurrent": {str(k): v[0] for k, v in sorted(by_k.items())},
                    "bootstrap_fit": "per-warp FP32 (the graph path)"},
         "sequential_plain": {"value": seq_steps / (seq_ms / 1e3), "ms_per_step": seq_ms,

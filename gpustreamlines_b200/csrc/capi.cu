@@ -1063,7 +1063,7 @@ struct csl_multi {
     cudaGraphExec_t exec = nullptr;
     std::vector<cudaEvent_t> tracked;  // end of each branch's tracking kernel (concurrency limit)
     std::vector<int> order;            // branch order: grouped by getter, larger batches first
-    int max_concurrent = 0;            // tracking kernels in flight at once (0: no limit)
+    int max_concurrent = 2;            // tracking kernels in flight at once (0: no limit)
     bool dirty = true, in_flight = false;
     int captures = 0;
     float ms = 0;
@@ -1263,7 +1263,7 @@ int csl_multi_create(csl_tracker *const *subjects, const float *const *seeds_dev
     m->br.assign(n_subjects, nullptr);
     m->join.assign(n_subjects, nullptr);
     m->tracked.assign(n_subjects, nullptr);
-    m->max_concurrent = 1;
+    m->max_concurrent = 2;
     m->order.resize(n_subjects);
     for (int i = 0; i < n_subjects; i++) m->order[i] = i;
     std::stable_sort(m->order.begin(), m->order.end(), [&](int a, int b) {

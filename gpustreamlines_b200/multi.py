@@ -80,6 +80,11 @@ class MultiSubjectRun:
         self.last = self.plan.wait()
         return self.last
 
+    def set_concurrency(self, max_concurrent: int):
+        """At most this many subjects' tracking kernels in flight (0: no limit,
+        default 2); takes effect at the next launch."""
+        self.plan.set_concurrency(max_concurrent)
+
     def run(self):
         self.launch()
         return self.wait()

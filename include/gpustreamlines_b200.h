@@ -332,7 +332,7 @@ int csl_multi_create(csl_tracker *const *subjects, const float *const *seeds_dev
 int csl_multi_launch(csl_multi *plan, void *stream);
 int csl_multi_wait(csl_multi *plan, long long *n_streamlines, long long *n_points, int *replayed, float *ms);
 int csl_multi_info(csl_multi *plan, int *captures, int *slot_caps, long long *pool_caps);
-/* At most max_concurrent tracking kernels in flight (0: no limit; default 1):
+/* At most max_concurrent tracking kernels in flight (0: no limit; default 2):
  * branches run grouped by getter, larger batches first, and each branch's
  * tracking kernel waits for the one max_concurrent places earlier; pass 1,
  * scans and compaction of the other branches still overlap.  Takes effect at
