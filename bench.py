@@ -14,6 +14,11 @@ direction + position update: steps = sum over streamlines of (length - 1).
   reference arm (--impl reference): the CPU restatement of the reference
           algorithm on all host threads, on a bounded sample of the same seeds
 
+Supplementary lines (not the headline): --getter (the other getters on the
+same phantom), --odf-volume (ODF/PMF volume generation), --learned (learned
+proposal), --multi (uneven subjects with mixed getters in one CUDA-graph
+launch against the same batches tracked one after another).
+
 Multi-GPU (torchrun): one process per GPU; each rank tracks its own 1M seeds
 (weak scaling, no data exchange); per-rank times are reduced with MAX and the
 per-rank streamline/point counts are all-gathered (the offsets a global TRX
