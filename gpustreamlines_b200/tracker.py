@@ -153,3 +153,24 @@ class GPUTracker(GenericTracker):
         logger.info("Destroying GPUTracker and freeing GPU memory...")
         self._release()
         return False
+
+    def autotune(self, seeds: np.ndarray, sample: int = 20000, repeats: int = 2, seed: int = 0):
+        """Choose the launch shape (threads per CTA, seed order) of every GPU's
+        tracking path by timing the candidates on a random sample of ``seeds``
+        (``csl_autotune``).  Streamlines do not depend on the shape.  Returns,
+        per GPU, {(threads_per_block, seed_order): ms or None} and the chosen shape."""
+        import torch
+
+        self._allocate()
+        seeds = np.ascontiguousarray(np.asarray(seeds, dtype=np.float32).reshape(-1, 3))
+        if len(seeds) == 0:
+            raise ValueError("autotune needs at least one seed")
+        rng = np.random.default_rng(seed)
+        pick = seeds[rng.choice(len(seeds), size=min(sample, len(seeds)), replace=False)]
+        out = []
+        for h in self.handles:
+            d = torch.from_numpy(np.ascontiguousarray(pick)).to(torch.device("cuda", h.device))
+            torch.cuda.synchronize(d.device)
+            ms = h.autotune(d.data_ptr(), len(pick), 0, repeats)
+            out.append((ms, h.get_launch()[:2]))
+        return out

@@ -202,3 +202,39 @@ def test_launch_shapes_do_not_change_streamlines(name, n):
             h.set_launch(96, 0)
     finally:
         h.close()
+
+
+def test_tracker_autotune_then_multi_subject_run():
+    """The reference-style API end to end: trackers tuned on their seeds, then
+    a MultiSubjectRun whose streamlines equal each tracker's own batch."""
+    import math
+
+    from gpustreamlines_b200 import ProbDirectionGetter, Tracker
+    from gpustreamlines_b200.multi import MultiSubjectRun
+    from oracle import cases
+
+    inp = cases.inputs("prob_s")
+    c = inp["case"]
+    trs, seeds = [], []
+    for k, n in enumerate((1500, 400)):
+        tr = Tracker(ProbDirectionGetter(), inp["dataf"], inp["stop_map"], c["fa_thr"], inp["vertices"],
+                     inp["edges"], max_angle=math.radians(c["max_angle"]), step_size=c["step"])
+        tr.__enter__()
+        trs.append(tr)
+        seeds.append(cases.seeds("prob_s", n, seed=50 + k))
+    try:
+        ref = []
+        for tr, s in zip(trs, seeds):
+            tr.handles[0].propagate(s)
+            ref.append(tr.handles[0].fetch())
+        (ms, shape), = trs[0].autotune(seeds[0], sample=1000, repeats=1)
+        assert ms[shape] is not None
+        with MultiSubjectRun(trs, seeds) as run:
+            nsl, npts, rep, _ = run.run()
+            for i in range(2):
+                for a, b in zip(run.results(i), ref[i]):
+                    assert np.array_equal(a, b)
+                assert len(run.streamlines(i)) == len(ref[i][0])
+    finally:
+        for tr in trs:
+            tr.__exit__(None, None, None)
