@@ -17,7 +17,8 @@ direction + position update: steps = sum over streamlines of (length - 1).
 Supplementary lines (not the headline): --getter (the other getters on the
 same phantom), --odf-volume (ODF/PMF volume generation), --learned (learned
 proposal), --multi (uneven subjects with mixed getters in one CUDA-graph
-launch against the same batches tracked one after another).
+launch against the same batches tracked one after another), --autotune (the
+launch-shape tuner's timings on the workload's seeds).
 
 Multi-GPU (torchrun): one process per GPU; each rank tracks its own 1M seeds
 (weak scaling, no data exchange); per-rank times are reduced with MAX and the
@@ -61,6 +62,8 @@ def parse():
     ap.add_argument("--multi", action="store_true",
                     help="multi-subject run: uneven subjects, mixed getters, one CUDA-graph launch")
     ap.add_argument("--subjects", type=int, default=12)
+    ap.add_argument("--autotune", action="store_true",
+                    help="print the launch-shape tuner's timings on this workload's seeds and exit")
     ap.add_argument("--learned", action="store_true",
                     help="train and evaluate the learned vMF-mixture proposal instead")
     ap.add_argument("--getter", default="prob", choices=sorted(GETTERS),
@@ -589,6 +592,16 @@ def main():
                       device_offset=local)
     tracker.__enter__()
     h = tracker.handles[0]
+    if args.autotune:
+        if rank == 0:
+            t0 = time.perf_counter()
+            ((ms, best),) = tracker.autotune(seeds, sample=len(seeds), repeats=2)
+            print(json.dumps({"workload": f"{gcfg['label']}, {args.seeds} seeds", "tuner_s": time.perf_counter() - t0,
+                              "batch_ms_by_shape": {f"{b} threads, {'Morton' if o else 'input'} order": v
+                                                    for (b, o), v in ms.items()},
+                              "chosen": {"threads_per_block": best[0], "seed_order": best[1]}}), flush=True)
+        tracker.__exit__(None, None, None)
+        return 0
     stream = torch.cuda.Stream(device=local)
     seeds_d = torch.from_numpy(seeds).to(f"cuda:{local}")
     seeds_pinned = torch.from_numpy(seeds).pin_memory()
