@@ -86,6 +86,10 @@ GETTERS = {
     # the headline workload
     "prob": dict(model="PROB", max_angle=45.0,
                  label="prob getter (plain FP32), 81x106x76 PMF x 724 vertices (1.9 GB)"),
+    # the same workload with the bounded-envelope sampler (bf16 cluster-maxima table)
+    "prob_env": dict(model="PROB", max_angle=45.0, sampler="envelope",
+                     label="prob getter, bounded-envelope rejection sampler (bf16 cluster-maxima table, "
+                           "exact PMF accept/reject), 81x106x76 PMF x 724 vertices (1.9 GB)"),
     # supplementary lines (not the headline): the other getters on the same phantom
     "csa": dict(model="CSA", max_angle=60.0, sh_order=8,
                 label="bootstrap CSA getter (plain FP32), sh_order 8 (45 coeffs), 81x106x76x160 DWI"),
@@ -128,7 +132,7 @@ def make_getter(getter: str, ph, sph):
                                                   fit=g.get("fit", "fp32"))
     if g["model"] == "PTT":
         return PttDirectionGetter()
-    return ProbDirectionGetter()
+    return ProbDirectionGetter(sampler=g.get("sampler", "inverse_cdf"))
 
 
 def measured_peaks():

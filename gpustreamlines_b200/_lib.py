@@ -40,7 +40,7 @@ class CslParams(C.Structure):
         ("probe_step_size", C.c_double), ("probe_quality", C.c_double),
         ("max_curvature", C.c_double),
         ("tile_log2_x", C.c_int), ("tile_log2_y", C.c_int),
-        ("tile_nx", C.c_int), ("tile_ny", C.c_int), ("tile_nz", C.c_int), ("_pad2", C.c_int),
+        ("tile_nx", C.c_int), ("tile_ny", C.c_int), ("tile_nz", C.c_int), ("prob_sampler", C.c_int),
     ]
 
 
@@ -70,7 +70,7 @@ EXPORTS = (
     "csl_mlp_adam", "csl_mlp_param_count", "csl_mlp_infer", "csl_dti_fa", "csl_seeds_from_mask",
     "csl_multi_create", "csl_multi_launch", "csl_multi_wait", "csl_multi_info", "csl_multi_destroy",
     "csl_multi_set_concurrency",
-    "csl_set_launch", "csl_get_launch", "csl_autotune",
+    "csl_set_launch", "csl_get_launch", "csl_autotune", "csl_sampler_stats", "csl_env_step",
 )
 
 
@@ -130,6 +130,8 @@ def load(path: str | None = None):
     lib.csl_set_launch.argtypes = [vp, C.c_int, C.c_int]
     lib.csl_get_launch.argtypes = [vp, _ip, _ip, _ip]
     lib.csl_autotune.argtypes = [vp, vp, ll, ll, C.c_int, _fp]
+    lib.csl_sampler_stats.argtypes = [vp, ull_p, C.c_int]
+    lib.csl_env_step.argtypes = [vp, _fp, _ip, _ip, ull_p, ll, _ip, _ip]
     lib.csl_last_error.argtypes = [vp, C.c_char_p, C.c_int]
     lib.csl_version.restype = C.c_char_p
     for name in EXPORTS:
@@ -323,6 +325,26 @@ class Handle:
                                         int(repeats), fptr(ms)))
         shapes = [(256, 0), (256, 1), (128, 0), (128, 1), (64, 0), (64, 1)]
         return {sh: (float(v) if v >= 0 else None) for sh, v in zip(shapes, ms)}
+
+    def sampler_stats(self, reset: bool = False):
+        """Envelope-sampler counters since creation or the last reset:
+        {steps, proposals, resolves, fallbacks}."""
+        out = np.zeros(4, dtype=np.uint64)
+        self._chk(self.lib.csl_sampler_stats(self.h, uptr(out), int(bool(reset))))
+        return dict(zip(("steps", "proposals", "resolves", "fallbacks"), (int(x) for x in out)))
+
+    def env_step(self, points, dir_vertex, dir_neg, subsequence):
+        """One envelope-sampler direction per query; returns (vertex or -1, sign)."""
+        pts = np.ascontiguousarray(points, dtype=np.float32).reshape(-1, 3)
+        n = len(pts)
+        dv = np.ascontiguousarray(dir_vertex, dtype=np.int32).reshape(n)
+        dn = np.ascontiguousarray(dir_neg, dtype=np.int32).reshape(n)
+        sq = np.ascontiguousarray(subsequence, dtype=np.uint64).reshape(n)
+        ov = np.zeros(n, dtype=np.int32)
+        on = np.zeros(n, dtype=np.int32)
+        self._chk(self.lib.csl_env_step(self.h, fptr(pts), iptr(dv), iptr(dn), uptr(sq), n, iptr(ov),
+                                        iptr(on)))
+        return ov, on
 
     def device_constants(self):
         a, b = C.c_float(), C.c_float()

@@ -64,6 +64,10 @@ struct csl_tracker {
     DevBuf<float> dataf, verts, H, R, delta_b, delta_q, sampling;
     DevBuf<int> edges, b0s, partner;
     DevBuf<uint32_t> cone, cone_t;
+    // bounded-envelope sampler (prob_sampler == 1)
+    DevBuf<uint32_t> env_cmax, env_cone;
+    DevBuf<short> env_member;
+    DevBuf<unsigned long long> env_stats;
     cudaArray_t stop_arr = nullptr, odf_arr = nullptr, lut_arr = nullptr;
     cudaTextureObject_t stop_tex = 0, odf_tex = 0, lut_tex = 0;
     DevBuf<float> consts;
@@ -230,6 +234,10 @@ static void release_all(csl_tracker *t) {
     for (auto *b : ib) b->release();
     t->cone.release();
     t->cone_t.release();
+    t->env_cmax.release();
+    t->env_cone.release();
+    t->env_member.release();
+    t->env_stats.release();
     t->peaks.release();
     t->out_src.release();
     t->pt_off.release();
@@ -269,7 +277,15 @@ static int validate(const csl_params *p, const csl_inputs *in, csl_tracker *t) {
         return fail(t, CSL_E_INVALID, "Invalid model type %d", p->model);
     if (p->dimx <= 0 || p->dimy <= 0 || p->dimz <= 0 || p->dimt <= 0)
         return fail(t, CSL_E_INVALID, "volume dimensions must be positive");
+    if ((long long)p->dimx * p->dimy * p->dimz >= (1LL << 31))
+        return fail(t, CSL_E_INVALID, "at most 2^31 - 1 voxels");
     if (p->nvertices <= 0 || p->nedges <= 0) return fail(t, CSL_E_INVALID, "empty sphere");
+    if (p->prob_sampler != 0 && p->prob_sampler != 1)
+        return fail(t, CSL_E_INVALID, "prob_sampler must be 0 or 1");
+    if (p->prob_sampler == 1 && p->model != CSL_MODEL_PROB)
+        return fail(t, CSL_E_INVALID, "prob_sampler=1 applies to the probabilistic getter only");
+    if (p->prob_sampler == 1 && p->dimt > 16 * 64)
+        return fail(t, CSL_E_INVALID, "prob_sampler=1 supports at most 1024 sphere vertices");
     if (p->nvertices > 32767) return fail(t, CSL_E_INVALID, "at most 32767 sphere vertices");
     if (p->max_sline_len < 2) return fail(t, CSL_E_INVALID, "max_sline_len must be >= 2");
     if (p->seed_order != 0 && p->seed_order != 1) return fail(t, CSL_E_INVALID, "seed_order must be 0 or 1");
@@ -472,6 +488,23 @@ int csl_create(const csl_params *params, const csl_inputs *inputs, int device, c
             P.cone_mask = t->cone.p;
             P.cone_mask_t = t->cone_t.p;
             CK(launch_cone_mask(P, t->cone.p, t->cone_t.p, t->own_stream));
+            if (p.prob_sampler == 1) {
+                std::vector<short> member;
+                if (!env_clusters(inputs->vertices, p.nvertices, member))
+                    return fail(t, CSL_E_INVALID, "prob_sampler=1: a vertex cluster exceeds %d vertices",
+                                kEnvMaxMembers);
+                if ((r = upload(t, t->env_member, member.data(), member.size()))) return r;
+                CK(t->env_cmax.ensure(nvox * kWarp));
+                CK(t->env_cone.ensure((size_t)2 * P.nvert * kEnvClusters));
+                CK(t->env_stats.ensure(4));
+                CK(cudaMemsetAsync(t->env_stats.p, 0, 4 * sizeof(unsigned long long), t->own_stream));
+                CK(launch_env_tables(P, t->env_member.p, t->env_cmax.p, t->env_cone.p, t->nsm, t->own_stream));
+                P.env = 1;
+                P.env_cmax = t->env_cmax.p;
+                P.env_cone = t->env_cone.p;
+                P.env_member = t->env_member.p;
+                P.env_stats = t->env_stats.p;
+            }
         }
         if (p.model == PTT) {
             r = make_texture3d(t, inputs->ptt_odf_tiled, p.tile_nx * p.dimx, p.tile_ny * p.dimy,
@@ -1002,6 +1035,57 @@ int csl_batch_timings(csl_tracker *t, float *ms4, int *pass2_runs) {
     if (ms4)
         for (int i = 0; i < 4; i++) ms4[i] = t->ms[i];
     if (pass2_runs) *pass2_runs = t->pass2_runs;
+    return CSL_OK;
+}
+
+int csl_sampler_stats(csl_tracker *t, unsigned long long *out4, int reset) {
+    if (!t) return fail(nullptr, CSL_E_INVALID, "NULL tracker");
+    if (!t->P.env) return fail(t, CSL_E_STATE, "the tracker does not use the envelope sampler (prob_sampler=1)");
+    CK(cudaSetDevice(t->device));
+    if (out4) {
+        CK(cudaMemcpyAsync(out4, t->env_stats.p, 4 * sizeof(unsigned long long), cudaMemcpyDeviceToHost,
+                           t->own_stream));
+    }
+    if (reset) CK(cudaMemsetAsync(t->env_stats.p, 0, 4 * sizeof(unsigned long long), t->own_stream));
+    CK(cudaStreamSynchronize(t->own_stream));
+    return CSL_OK;
+}
+
+int csl_env_step(csl_tracker *t, const float *points, const int *dir_vertex, const int *dir_neg,
+                 const unsigned long long *subsequence, long long n, int *out_vertex, int *out_neg) {
+    if (!t) return fail(nullptr, CSL_E_INVALID, "NULL tracker");
+    if (!t->P.env) return fail(t, CSL_E_STATE, "the tracker does not use the envelope sampler (prob_sampler=1)");
+    if (n < 0 || n > (1LL << 30) ||
+        (n > 0 && (!points || !dir_vertex || !dir_neg || !subsequence || !out_vertex || !out_neg)))
+        return fail(t, CSL_E_INVALID, "bad arguments");
+    for (long long i = 0; i < n; i++)
+        if (dir_vertex[i] < 0 || dir_vertex[i] >= t->P.nvert || (dir_neg[i] != 0 && dir_neg[i] != 1))
+            return fail(t, CSL_E_INVALID, "query %lld: direction must be +/- a sphere vertex", i);
+    if (n == 0) return CSL_OK;
+    CK(cudaSetDevice(t->device));
+    cudaStream_t st = t->own_stream;
+    const int ni = (int)n;
+    DevBuf<float> pd;
+    DevBuf<int> dv, dn, ov, on;
+    DevBuf<unsigned long long> sq;
+    cudaError_t e = cudaSuccess;
+    auto step = [&](cudaError_t x) { if (e == cudaSuccess) e = x; };
+    step(pd.ensure((size_t)ni * 3));
+    step(dv.ensure(ni));
+    step(dn.ensure(ni));
+    step(ov.ensure(ni));
+    step(on.ensure(ni));
+    step(sq.ensure(ni));
+    step(cudaMemcpyAsync(pd.p, points, (size_t)ni * 12, cudaMemcpyHostToDevice, st));
+    step(cudaMemcpyAsync(dv.p, dir_vertex, (size_t)ni * 4, cudaMemcpyHostToDevice, st));
+    step(cudaMemcpyAsync(dn.p, dir_neg, (size_t)ni * 4, cudaMemcpyHostToDevice, st));
+    step(cudaMemcpyAsync(sq.p, subsequence, (size_t)ni * 8, cudaMemcpyHostToDevice, st));
+    step(launch_env_step(t->P, pd.p, dv.p, dn.p, sq.p, ni, ov.p, on.p, st));
+    step(cudaMemcpyAsync(out_vertex, ov.p, (size_t)ni * 4, cudaMemcpyDeviceToHost, st));
+    step(cudaMemcpyAsync(out_neg, on.p, (size_t)ni * 4, cudaMemcpyDeviceToHost, st));
+    step(cudaStreamSynchronize(st));
+    pd.release(); dv.release(); dn.release(); ov.release(); on.release(); sq.release();
+    CK(e);
     return CSL_OK;
 }
 

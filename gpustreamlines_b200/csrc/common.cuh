@@ -45,6 +45,12 @@ struct DevParams {
     cudaTextureObject_t stop_tex;        // stop map, border -1, linear filter
     const uint32_t *__restrict__ cone_mask;    // PROB: [2][V][nch] keep bits
     const uint32_t *__restrict__ cone_mask_t;  // PROB: [2][V][32] the same bits, per lane
+    // PROB with the bounded-envelope sampler (env != 0; envelope.cuh)
+    int env;
+    const uint32_t *__restrict__ env_cmax;    // [X*Y*Z][32]: cluster maxima rounded up to bf16, 2 per word
+    const uint32_t *__restrict__ env_cone;    // [2][V][64]: cone bits of each cluster's members
+    const short *__restrict__ env_member;     // [64][32]: vertex ids of each cluster (-1 padded)
+    unsigned long long *env_stats;            // [4] counters: steps, proposals, exact resolutions, fallbacks
     // bootstrap
     float min_signal;
     int delta_nr, hr_side;
@@ -112,7 +118,9 @@ struct Corners {
     float w[8];         // ((wx*wy)*wz) in (i,j,k) lexicographic order
 };
 
-__device__ __forceinline__ bool trilinear_setup(const DevParams &P, float3 p, Corners &c) {
+// Corner voxels (flat index (x*Y + y)*Z + z) and weights of the trilinear
+// interpolation at p; false outside the volume.
+__device__ __forceinline__ bool trilinear_vox(const DevParams &P, float3 p, int (&vox)[8], float (&w)[8]) {
     const float HALF = 0.5f;
     if (!(p.x == p.x) || !(p.y == p.y) || !(p.z == p.z)) return false;
     if (p.x < -HALF || p.x + HALF >= (float)P.dimx || p.y < -HALF || p.y + HALF >= (float)P.dimy ||
@@ -120,20 +128,19 @@ __device__ __forceinline__ bool trilinear_setup(const DevParams &P, float3 p, Co
         return false;
     const float flx = floorf(p.x), fly = floorf(p.y), flz = floorf(p.z);
     float wgh[3][2];
-    long long coo[3][2];
+    int coo[3][2];
     wgh[0][1] = p.x - flx;
     wgh[0][0] = 1.0f - wgh[0][1];
-    coo[0][0] = (long long)((0 > flx) ? 0 : flx);
+    coo[0][0] = (int)((0 > flx) ? 0 : flx);
     coo[0][1] = ((P.dimx - 1) < coo[0][0] + 1) ? (P.dimx - 1) : coo[0][0] + 1;
     wgh[1][1] = p.y - fly;
     wgh[1][0] = 1.0f - wgh[1][1];
-    coo[1][0] = (long long)((0 > fly) ? 0 : fly);
+    coo[1][0] = (int)((0 > fly) ? 0 : fly);
     coo[1][1] = ((P.dimy - 1) < coo[1][0] + 1) ? (P.dimy - 1) : coo[1][0] + 1;
     wgh[2][1] = p.z - flz;
     wgh[2][0] = 1.0f - wgh[2][1];
-    coo[2][0] = (long long)((0 > flz) ? 0 : flz);
+    coo[2][0] = (int)((0 > flz) ? 0 : flz);
     coo[2][1] = ((P.dimz - 1) < coo[2][0] + 1) ? (P.dimz - 1) : coo[2][0] + 1;
-    const long long T = P.dimt, ZT = (long long)P.dimz * T, YZT = (long long)P.dimy * ZT;
 #pragma unroll
     for (int i = 0; i < 2; i++)
 #pragma unroll
@@ -141,9 +148,17 @@ __device__ __forceinline__ bool trilinear_setup(const DevParams &P, float3 p, Co
 #pragma unroll
             for (int k = 0; k < 2; k++) {
                 const int q = (i << 2) | (j << 1) | k;
-                c.base[q] = coo[0][i] * YZT + coo[1][j] * ZT + coo[2][k] * T;
-                c.w[q] = wgh[0][i] * wgh[1][j] * wgh[2][k];
+                vox[q] = (coo[0][i] * P.dimy + coo[1][j]) * P.dimz + coo[2][k];
+                w[q] = wgh[0][i] * wgh[1][j] * wgh[2][k];
             }
+    return true;
+}
+
+__device__ __forceinline__ bool trilinear_setup(const DevParams &P, float3 p, Corners &c) {
+    int vox[8];
+    if (!trilinear_vox(P, p, vox, c.w)) return false;
+#pragma unroll
+    for (int q = 0; q < 8; q++) c.base[q] = (long long)vox[q] * P.dimt;
     return true;
 }
 

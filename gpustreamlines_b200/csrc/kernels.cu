@@ -23,14 +23,6 @@
 #include "ptt.cuh"
 #include "track.cuh"
 
-// resident 256-thread blocks per SM the probabilistic tracker is compiled for
-#ifndef CSL_BOOT_MIN_BLOCKS
-#define CSL_BOOT_MIN_BLOCKS 2
-#endif
-#ifndef CSL_PROB_MIN_BLOCKS
-#define CSL_PROB_MIN_BLOCKS 4
-#endif
-
 namespace csl {
 
 __host__ int smem_bytes(const DevParams &P, int warps, bool track) {
@@ -66,24 +58,6 @@ __global__ void __launch_bounds__(256) seed_peaks_kernel(DevParams P, const floa
 // ---------------------------------------------------------------------------
 // pass 2: tracking
 
-// Next seed for the calling warp (lane 0).  Input order: one global counter.
-// Spatial order: the seeds are sorted by the Morton code of their voxel and
-// each block owns a contiguous range of that order, so the warps of a block
-// track neighbouring seeds at the same time and share voxel rows in L1; a
-// block whose range is exhausted takes positions from the following blocks'
-// ranges.  Every position is claimed exactly once; results do not depend on
-// the order.
-__device__ __forceinline__ int next_seed(const BatchArgs &B) {
-    if (!B.perm) return atomicAdd(B.queue, 1);
-    const int nb = gridDim.x;
-    for (int k = 0; k < nb; k++) {
-        const int b = (blockIdx.x + k) % nb;
-        const int p = atomicAdd(B.blk_next + b, 1);
-        if (p < B.blk_end[b]) return B.perm[p];
-    }
-    return B.nseeds;
-}
-
 // 30-bit Morton code of each seed's voxel (10 bits per axis)
 __device__ __forceinline__ uint32_t spread3(uint32_t v) {
     v &= 0x3ffu;
@@ -111,102 +85,6 @@ __global__ void block_ranges_kernel(int n, int nblocks, int *next, int *end) {
     if (b >= nblocks) return;
     next[b] = (int)((long long)n * b / nblocks);
     end[b] = (int)((long long)n * (b + 1) / nblocks);
-}
-
-template <int MODEL>
-__global__ void __launch_bounds__(256, MODEL == PROB ? CSL_PROB_MIN_BLOCKS
-                                         : (MODEL == PTT ? 1 : CSL_BOOT_MIN_BLOCKS)) track_kernel(DevParams P, BatchArgs B, const int *partner,
-                                                    const int *__restrict__ npeaks,
-                                                    const short *__restrict__ peaks, int max_store,
-                                                    const int *__restrict__ sl_off, int *out_len,
-                                                    int *out_seed, long long *out_src) {
-    extern __shared__ float smem[];
-    int *partner_sh = reinterpret_cast<int *>(smem);
-    load_partner(partner, partner_sh);
-    __syncthreads();
-    const int warp = threadIdx.x / kWarp, lane = threadIdx.x & 31;
-    const size_t gwarp = (size_t)blockIdx.x * (blockDim.x / kWarp) + warp;
-    float *scrB = B.scratch + gwarp * (size_t)scratch_floats_per_warp(P);
-    float *scrF = scrB + (size_t)P.max_sline_len * 3;
-    int *plist = reinterpret_cast<int *>(scrF + (size_t)P.max_sline_len * 3);
-    const WarpBufs W = carve(P, smem + kMaxSortLayers * kWarp, warp, true, plist);
-
-    for (;;) {
-        int s = 0;
-        if (lane == 0) s = next_seed(B);
-        s = __shfl_sync(FULL, s, 0);
-        if (s >= B.nseeds) break;
-        const int np = npeaks[s];
-        if (np == 0) continue;
-        const int base = sl_off[s];
-        if (base + np > B.sl_cap) {
-            if (lane == 0) atomicOr(B.status, ST_SLOT_OVERFLOW);
-            continue;
-        }
-        const float3 seed = make_float3(B.seeds[3 * s], B.seeds[3 * s + 1], B.seeds[3 * s + 2]);
-        const unsigned long long gid = 32ull * (unsigned long long)(s + B.rng_index_base) + lane;
-        // peak list: stored by pass 1, or recomputed into this warp's scratch
-        const short *stored = peaks + (size_t)s * max_store;
-        if (np > max_store) {
-            seed_peaks_dispatch<MODEL>(P, seed, W, partner_sh, lane, gid);
-            if (W.ind != plist)
-                for (int k = lane; k < np; k += kWarp) plist[k] = W.ind[k];
-        }
-        __syncwarp();
-        typename RngOf<MODEL>::T rng;
-        if constexpr (MODEL == PROB) rng.st = W.rng;
-        rng.init(P.rng_seed, gid + 1, 0);
-        {
-            for (int k = 0; k < np; k++) {
-                const int pv = (np > max_store) ? plist[k] : (int)stored[k];
-                const float3 fs = vert3(P.verts, pv);
-                int len;
-                int nB = 0, nF = 0;
-                bool single = false;
-                if constexpr (MODEL == PTT) {
-                    PttSmem S{W.face, W.vpdf};
-                    if (!ptt_init_frame(P, rng, fs, seed, W.frame, S, lane)) single = true;
-                }
-                if (single) {
-                    if (lane == 0) store_pt(scrB, 0, seed);
-                    __syncwarp();
-                    nB = 1;
-                    nF = 1;
-                    len = 1;
-                } else {
-                    DirState db{make_float3(-fs.x, -fs.y, -fs.z), pv, 1};
-                    DirState df{fs, pv, 0};
-                    nB = track_one<MODEL>(P, rng, seed, db, W.frame, scrB, W, partner_sh, lane);
-                    nF = track_one<MODEL>(P, rng, seed, df, W.frame + 9, scrF, W, partner_sh,
-                                                 lane);
-                    len = nB - 1 + nF;
-                }
-                __syncwarp();
-                unsigned long long off = 0;
-                if (lane == 0) off = atomicAdd(B.pool_count, (unsigned long long)len);
-                off = __shfl_sync(FULL, off, 0);
-                long long src = -1;
-                if (off + (unsigned long long)len <= B.pool_cap) {
-                    src = (long long)off;
-                    float *dst = B.pool + off * 3;
-                    for (int j = lane; j < len; j += kWarp) {
-                        const float *p = (j < nB) ? scrB + 3 * (nB - 1 - j) : scrF + 3 * (j - nB + 1);
-                        dst[3 * j] = p[0];
-                        dst[3 * j + 1] = p[1];
-                        dst[3 * j + 2] = p[2];
-                    }
-                } else if (lane == 0) {
-                    atomicOr(B.status, ST_POOL_OVERFLOW);
-                }
-                if (lane == 0) {
-                    out_len[base + k] = len;
-                    out_seed[base + k] = s;
-                    out_src[base + k] = src;
-                }
-                __syncwarp();
-            }
-        }
-    }
 }
 
 // ---------------------------------------------------------------------------
@@ -416,6 +294,7 @@ cudaError_t launch_seed_peaks(const DevParams &P, const float *seeds, int n, lon
 }
 
 cudaError_t track_occupancy(const DevParams &P, int block, int *blocks_per_sm) {
+    if (P.env) return track_occupancy_env(P, block, blocks_per_sm);
     const int smem = smem_bytes(P, block / kWarp, true);
     cudaError_t e = cudaSuccess;
     CSL_DISPATCH_MODEL(P.model, {
@@ -431,6 +310,9 @@ cudaError_t launch_track(const DevParams &P, const BatchArgs &B, const int *part
                          const int *npeaks, const short *peaks, int max_store, const int *sl_off,
                          int *out_len, int *out_seed, long long *out_src, int grid, int block,
                          cudaStream_t st) {
+    if (P.env)
+        return launch_track_env(P, B, partner, npeaks, peaks, max_store, sl_off, out_len, out_seed, out_src,
+                                grid, block, st);
     const int smem = smem_bytes(P, block / kWarp, true);
     cudaError_t e = cudaSuccess;
     CSL_DISPATCH_MODEL(P.model, {

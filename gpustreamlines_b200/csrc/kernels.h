@@ -2,6 +2,7 @@
 #pragma once
 #include <cstddef>
 #include <cstdint>
+#include <vector>
 #include <cuda_runtime.h>
 
 #include "common.cuh"
@@ -26,6 +27,19 @@ cudaError_t launch_track(const DevParams &P, const BatchArgs &B, const int *part
                          const int *npeaks, const short *peaks, int max_store, const int *sl_off,
                          int *out_len, int *out_seed, long long *out_src, int grid, int block,
                          cudaStream_t st);
+// ---- probabilistic tracking with the bounded-envelope sampler (envelope.cu)
+constexpr int kEnvClusters = 64;    // vertex clusters: two per lane
+constexpr int kEnvMaxMembers = 32;  // vertices per cluster (one 32-bit cone word)
+bool env_clusters(const float *verts, int V, std::vector<short> &member);
+cudaError_t launch_env_tables(const DevParams &P, const short *member, uint32_t *cmax, uint32_t *cone,
+                              int nsm, cudaStream_t st);
+cudaError_t track_occupancy_env(const DevParams &P, int block, int *blocks_per_sm);
+cudaError_t launch_track_env(const DevParams &P, const BatchArgs &B, const int *partner, const int *npeaks,
+                             const short *peaks, int max_store, const int *sl_off, int *out_len, int *out_seed,
+                             long long *out_src, int grid, int block, cudaStream_t st);
+cudaError_t launch_env_step(const DevParams &P, const float *pts, const int *dir_vtx, const int *dir_neg,
+                            const unsigned long long *subseq, int n, int *out_vtx, int *out_neg,
+                            cudaStream_t st);
 cudaError_t launch_get_direction(const DevParams &P, const int *partner, const float *pts,
                                  const float *dirs, const unsigned long long *subseq,
                                  const unsigned long long *offs, int n, float *frames,

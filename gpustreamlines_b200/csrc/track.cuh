@@ -5,9 +5,19 @@
 #pragma once
 #include "boot.cuh"
 #include "common.cuh"
+#include "envelope.cuh"
 #include "kernels.h"
 #include "prob.cuh"
 #include "ptt.cuh"
+
+// resident 256-thread blocks per SM the probabilistic tracker is compiled for
+#ifndef CSL_BOOT_MIN_BLOCKS
+#define CSL_BOOT_MIN_BLOCKS 2
+#endif
+#ifndef CSL_PROB_MIN_BLOCKS
+#define CSL_PROB_MIN_BLOCKS 4
+#endif
+
 
 namespace csl {
 
@@ -96,9 +106,18 @@ __device__ __forceinline__ int seed_peaks_dispatch(const DevParams &P, float3 se
 // ---------------------------------------------------------------------------
 // pass 2: tracking
 
+// Template tag of the probabilistic tracker with the bounded-envelope sampler
+// (P.model stays PROB; envelope.cuh).
+constexpr int PROB_ENV = 4;
+__host__ __device__ constexpr int base_model(int m) { return m == PROB_ENV ? PROB : m; }
+
 template <int MODEL>
 struct RngOf {
     using T = Philox;
+};
+template <>
+struct RngOf<PROB_ENV> {
+    using T = PhiloxShared;
 };
 template <>
 struct RngOf<PROB> {
@@ -119,8 +138,9 @@ __device__ __forceinline__ void store_pt(float *out, int i, float3 p) {
 template <int MODEL>
 __device__ __forceinline__ int track_one(const DevParams &P, typename RngOf<MODEL>::T &rng, float3 seed,
                          DirState dir, float *frame, float *out, const WarpBufs &W,
-                         const int *partner_sh, int lane) {
+                         const int *partner_sh, int lane, EnvCount &cnt) {
     if constexpr (MODEL == PROB) return prob_track(P, rng, seed, dir, out, W.odf, lane);
+    if constexpr (MODEL == PROB_ENV) return prob_env_track(P, rng, seed, dir, out, W.odf, lane, cnt);
     const int step_frac = (MODEL == PTT) ? P.step_frac : 1;
     const double ss = P.step_size / step_frac;
     float3 pt = seed;
@@ -132,13 +152,13 @@ __device__ __forceinline__ int track_one(const DevParams &P, typename RngOf<MODE
         DirState nd;
         nd.vtx = -1;
         nd.neg = 0;
-        int ndir;
+        int ndir = 0;
         if constexpr (MODEL == PROB) {
             ndir = prob_get_direction(P, pt, dir, W.odf, rng, lane, &nd, nullptr);
         } else if constexpr (MODEL == PTT) {
             PttSmem S{W.face, W.vpdf};
             ndir = ptt_get_direction<false>(P, rng, dir.d, frame, pt, S, lane, &nd.d);
-        } else {
+        } else if constexpr (MODEL == OPDT || MODEL == CSA) {
             BootSmem S{W.vox, W.msk, W.r, W.h, W.ind};
             ndir = boot_get_direction<5, MODEL>(P, rng, dir.d, pt, S, partner_sh, lane, &nd.d,
                                                 nullptr);
@@ -158,5 +178,126 @@ __device__ __forceinline__ int track_one(const DevParams &P, typename RngOf<MODE
     return nsteps;
 }
 
+
+// ---------------------------------------------------------------------------
+// pass 2: the persistent tracking kernel
+
+// Next seed for the calling warp (lane 0).  Input order: one global counter.
+// Spatial order: the seeds are sorted by the Morton code of their voxel and
+// each block owns a contiguous range of that order, so the warps of a block
+// track neighbouring seeds at the same time and share voxel rows in L1; a
+// block whose range is exhausted takes positions from the following blocks'
+// ranges.  Every position is claimed exactly once; results do not depend on
+// the order.
+__device__ __forceinline__ int next_seed(const BatchArgs &B) {
+    if (!B.perm) return atomicAdd(B.queue, 1);
+    const int nb = gridDim.x;
+    for (int k = 0; k < nb; k++) {
+        const int b = (blockIdx.x + k) % nb;
+        const int p = atomicAdd(B.blk_next + b, 1);
+        if (p < B.blk_end[b]) return B.perm[p];
+    }
+    return B.nseeds;
+}
+
+template <int MODEL>
+__global__ void __launch_bounds__(256, base_model(MODEL) == PROB ? CSL_PROB_MIN_BLOCKS
+                                         : (MODEL == PTT ? 1 : CSL_BOOT_MIN_BLOCKS)) track_kernel(DevParams P, BatchArgs B, const int *partner,
+                                                    const int *__restrict__ npeaks,
+                                                    const short *__restrict__ peaks, int max_store,
+                                                    const int *__restrict__ sl_off, int *out_len,
+                                                    int *out_seed, long long *out_src) {
+    extern __shared__ float smem[];
+    int *partner_sh = reinterpret_cast<int *>(smem);
+    load_partner(partner, partner_sh);
+    __syncthreads();
+    const int warp = threadIdx.x / kWarp, lane = threadIdx.x & 31;
+    const size_t gwarp = (size_t)blockIdx.x * (blockDim.x / kWarp) + warp;
+    float *scrB = B.scratch + gwarp * (size_t)scratch_floats_per_warp(P);
+    float *scrF = scrB + (size_t)P.max_sline_len * 3;
+    int *plist = reinterpret_cast<int *>(scrF + (size_t)P.max_sline_len * 3);
+    const WarpBufs W = carve(P, smem + kMaxSortLayers * kWarp, warp, true, plist);
+    EnvCount cnt = {0, 0, 0, 0};
+
+    for (;;) {
+        int s = 0;
+        if (lane == 0) s = next_seed(B);
+        s = __shfl_sync(FULL, s, 0);
+        if (s >= B.nseeds) {
+            if constexpr (MODEL == PROB_ENV) env_flush(P, cnt, lane);
+            break;
+        }
+        const int np = npeaks[s];
+        if (np == 0) continue;
+        const int base = sl_off[s];
+        if (base + np > B.sl_cap) {
+            if (lane == 0) atomicOr(B.status, ST_SLOT_OVERFLOW);
+            continue;
+        }
+        const float3 seed = make_float3(B.seeds[3 * s], B.seeds[3 * s + 1], B.seeds[3 * s + 2]);
+        const unsigned long long gid = 32ull * (unsigned long long)(s + B.rng_index_base) + lane;
+        // peak list: stored by pass 1, or recomputed into this warp's scratch
+        const short *stored = peaks + (size_t)s * max_store;
+        if (np > max_store) {
+            seed_peaks_dispatch<base_model(MODEL)>(P, seed, W, partner_sh, lane, gid);
+            if (W.ind != plist)
+                for (int k = lane; k < np; k += kWarp) plist[k] = W.ind[k];
+        }
+        __syncwarp();
+        typename RngOf<MODEL>::T rng;
+        if constexpr (base_model(MODEL) == PROB) rng.st = W.rng;
+        rng.init(P.rng_seed, gid + 1, 0);
+        {
+            for (int k = 0; k < np; k++) {
+                const int pv = (np > max_store) ? plist[k] : (int)stored[k];
+                const float3 fs = vert3(P.verts, pv);
+                int len;
+                int nB = 0, nF = 0;
+                bool single = false;
+                if constexpr (MODEL == PTT) {
+                    PttSmem S{W.face, W.vpdf};
+                    if (!ptt_init_frame(P, rng, fs, seed, W.frame, S, lane)) single = true;
+                }
+                if (single) {
+                    if (lane == 0) store_pt(scrB, 0, seed);
+                    __syncwarp();
+                    nB = 1;
+                    nF = 1;
+                    len = 1;
+                } else {
+                    DirState db{make_float3(-fs.x, -fs.y, -fs.z), pv, 1};
+                    DirState df{fs, pv, 0};
+                    nB = track_one<MODEL>(P, rng, seed, db, W.frame, scrB, W, partner_sh, lane, cnt);
+                    nF = track_one<MODEL>(P, rng, seed, df, W.frame + 9, scrF, W, partner_sh,
+                                                 lane, cnt);
+                    len = nB - 1 + nF;
+                }
+                __syncwarp();
+                unsigned long long off = 0;
+                if (lane == 0) off = atomicAdd(B.pool_count, (unsigned long long)len);
+                off = __shfl_sync(FULL, off, 0);
+                long long src = -1;
+                if (off + (unsigned long long)len <= B.pool_cap) {
+                    src = (long long)off;
+                    float *dst = B.pool + off * 3;
+                    for (int j = lane; j < len; j += kWarp) {
+                        const float *p = (j < nB) ? scrB + 3 * (nB - 1 - j) : scrF + 3 * (j - nB + 1);
+                        dst[3 * j] = p[0];
+                        dst[3 * j + 1] = p[1];
+                        dst[3 * j + 2] = p[2];
+                    }
+                } else if (lane == 0) {
+                    atomicOr(B.status, ST_POOL_OVERFLOW);
+                }
+                if (lane == 0) {
+                    out_len[base + k] = len;
+                    out_seed[base + k] = s;
+                    out_src[base + k] = src;
+                }
+                __syncwarp();
+            }
+        }
+    }
+}
 
 }  // namespace csl

@@ -121,12 +121,20 @@ class ProbDirectionGetter(GPUDirectionGetter):
 
     model = _lib.MODEL_PROB
 
-    def __init__(self):
-        pass
+    def __init__(self, *, sampler: str = "inverse_cdf"):
+        """``sampler`` (keyword only, not in the reference): "inverse_cdf" is
+        the reference's sampler with identical results; "envelope" draws from
+        the same distribution by exact rejection sampling, with proposals
+        bounded by per-voxel vertex-cluster maxima (bfloat16, rounded up), and
+        falls back to the inverse CDF after 16 rejected proposals."""
+        if sampler not in ("inverse_cdf", "envelope"):
+            raise ValueError(f"Invalid sampler {sampler!r}, must be one of 'inverse_cdf', 'envelope'")
+        self.sampler = sampler
 
     def fill(self, params, inputs, tracker, keep):
         params.model = _lib.MODEL_PROB
         params.samplm_nr = tracker.dimt
+        params.prob_sampler = 1 if self.sampler == "envelope" else 0
 
 
 class PttDirectionGetter(ProbDirectionGetter):

@@ -79,7 +79,13 @@ typedef struct csl_params {
     double max_curvature;         /* MAX_CURVATURE = 8 sin(max_angle / 2) */
     int tile_log2_x, tile_log2_y; /* PTT ODF texture tiling (LOG2_X, LOG2_Y) */
     int tile_nx, tile_ny, tile_nz;/* tiles per axis (nx, ny, nz) */
-    int _pad2;
+    int prob_sampler;             /* probabilistic getter's sampler: 0 = inverse CDF over the whole
+                                     PMF, the reference's (get_direction_prob_d,
+                                     generate_streamlines_cuda.cu:54-275; results identical to it);
+                                     1 = exact rejection sampler of the same distribution with a
+                                     proposal bounded by per-voxel vertex-cluster maxima (no
+                                     counterpart in the reference; same distribution, different
+                                     random draws, so streamlines differ individually) */
 } csl_params;
 
 /*
@@ -357,6 +363,28 @@ int csl_set_launch(csl_tracker *t, int threads_per_block, int seed_order);
 int csl_get_launch(csl_tracker *t, int *threads_per_block, int *seed_order, int *blocks_per_sm);
 int csl_autotune(csl_tracker *t, const float *seeds_dev, long long n, long long rng_index_base, int repeats,
                  float *ms_out);
+
+/*
+ * Bounded-envelope sampler of the probabilistic getter (prob_sampler = 1; no
+ * counterpart in the reference, whose sampler is the inverse CDF of
+ * get_direction_prob_d, generate_streamlines_cuda.cu:54-275).
+ *   csl_sampler_stats  out4 = {steps sampled, proposals drawn, proposals whose
+ *                      threshold test needed the exact maximum (corner rows
+ *                      gathered), steps finished by the inverse-CDF fallback}
+ *                      accumulated over batches since creation or the last
+ *                      reset (reset != 0 zeroes them after reading).
+ *   csl_env_step       one direction per query with the sampler (test entry
+ *                      point, like csl_get_direction): query i at points[i],
+ *                      incoming direction (-1)^dir_neg[i] * vertex
+ *                      dir_vertex[i], lane 0's Philox stream at
+ *                      (rng_seed, subsequence[i], offset 0).  out_vertex[i] =
+ *                      the sampled vertex or -1 when the getter stops;
+ *                      out_neg[i] = 1 when the returned direction is its
+ *                      negation.  Host arrays.
+ */
+int csl_sampler_stats(csl_tracker *t, unsigned long long *out4, int reset);
+int csl_env_step(csl_tracker *t, const float *points, const int *dir_vertex, const int *dir_neg,
+                 const unsigned long long *subsequence, long long n, int *out_vertex, int *out_neg);
 
 const char *csl_version(void);
 

@@ -33,7 +33,7 @@ from conftest import ROOT
 pytestmark = pytest.mark.gpu
 
 
-def _handle(name, inp=None, seed_order=0, boot_fit=0):
+def _handle(name, inp=None, seed_order=0, boot_fit=0, prob_sampler=0):
     from gpustreamlines_b200 import _lib
     from oracle import cases
 
@@ -54,6 +54,7 @@ def _handle(name, inp=None, seed_order=0, boot_fit=0):
     p.rng_seed = int(c["rng_seed"])
     p.seed_order = seed_order
     p.boot_fit = boot_fit
+    p.prob_sampler = prob_sampler
     p.sphere_symm = int(c.get("sphere_symm", 0))
     ins = _lib.CslInputs()
     ins.stop_map = _lib.fptr(inp["stop_map"])
