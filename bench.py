@@ -48,6 +48,8 @@ BYTES_PER_STEP = 8 * 724 * 4 + 8 * 4 + 12  # PMF corners + stop-map taps + point
 # capture of this workload at 20,000 seeds (27.25 GB over 6,372,721 steps, see
 # profiles/track_kernel_prob_81x106x76x724.md); scaled to a full launch by steps.
 TRAFFIC_BYTES_PER_STEP = 4277.0
+# The same for track_kernel<PROB_ENV> (envelope sampler); 0 until captured.
+ENV_TRAFFIC_BYTES_PER_STEP = 0.0
 
 
 def parse():
@@ -66,10 +68,15 @@ def parse():
                     help="print the launch-shape tuner's timings on this workload's seeds and exit")
     ap.add_argument("--learned", action="store_true",
                     help="train and evaluate the learned vMF-mixture proposal instead")
-    ap.add_argument("--getter", default="prob", choices=sorted(GETTERS),
-                    help="prob = the headline workload; csa/opdt/ptt print supplementary lines")
+    ap.add_argument("--getter", default="prob_env", choices=sorted(GETTERS),
+                    help="prob_env = the headline (envelope sampler, with the plain FP32 kernel timed "
+                         "beside it); prob/csa/opdt/ptt/... print supplementary lines")
+    ap.add_argument("--no-plain-arm", action="store_true",
+                    help="headline only: skip timing the plain FP32 inverse-CDF kernel beside it")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--env-traffic-bytes-per-step", type=float, default=ENV_TRAFFIC_BYTES_PER_STEP,
+                    help="DRAM bytes per step of the envelope-sampler kernel from an ncu capture (0 = unknown)")
     ap.add_argument("--traffic-bytes-per-step", type=float, default=TRAFFIC_BYTES_PER_STEP,
                     help="DRAM bytes per tracking step from an ncu capture (0 = unknown)")
     return ap.parse_args()
@@ -83,13 +90,16 @@ def dist_info():
 
 
 GETTERS = {
-    # the headline workload
-    "prob": dict(model="PROB", max_angle=45.0,
-                 label="prob getter (plain FP32), 81x106x76 PMF x 724 vertices (1.9 GB)"),
-    # the same workload with the bounded-envelope sampler (bf16 cluster-maxima table)
+    # the headline workload: probabilistic getter with the bounded-envelope
+    # proposal (bf16 cluster-maxima table, exact accept/reject against the FP32
+    # PMF); the plain FP32 inverse-CDF kernel is timed beside it in the same run
     "prob_env": dict(model="PROB", max_angle=45.0, sampler="envelope",
-                     label="prob getter, bounded-envelope rejection sampler (bf16 cluster-maxima table, "
-                           "exact PMF accept/reject), 81x106x76 PMF x 724 vertices (1.9 GB)"),
+                     label="prob getter, bounded-envelope proposal (bf16 cluster-maxima table) with exact FP32 "
+                           "PMF accept/reject, vs the plain FP32 inverse-CDF kernel; 81x106x76 PMF x 724 "
+                           "vertices (1.9 GB)"),
+    # the plain FP32 kernel alone (the reference's sampler, bit-exact to it)
+    "prob": dict(model="PROB", max_angle=45.0,
+                 label="prob getter (plain FP32 inverse CDF), 81x106x76 PMF x 724 vertices (1.9 GB)"),
     # supplementary lines (not the headline): the other getters on the same phantom
     "csa": dict(model="CSA", max_angle=60.0, sh_order=8,
                 label="bootstrap CSA getter (plain FP32), sh_order 8 (45 coeffs), 81x106x76x160 DWI"),
@@ -133,6 +143,45 @@ def make_getter(getter: str, ph, sph):
     if g["model"] == "PTT":
         return PttDirectionGetter()
     return ProbDirectionGetter(sampler=g.get("sampler", "inverse_cdf"))
+
+
+def plain_arm(args, data, ph, sph, gcfg, seeds_d, local, stream, barrier, dist, world):
+    """The plain FP32 inverse-CDF kernel on the same PMF and seeds, timed the same
+    way (device-resident seeds, pass 1 + pass 2 + compaction, max over ranks)."""
+    import torch
+
+    from gpustreamlines_b200 import ProbDirectionGetter, Tracker
+
+    with Tracker(ProbDirectionGetter(), data, ph.fa, 0.1, sph.vertices, sph.edges,
+                 max_angle=math.radians(gcfg["max_angle"]), step_size=0.5, ngpus=1, device_offset=local) as tr:
+        hp = tr.handles[0]
+        n = int(seeds_d.shape[0])
+        for _ in range(max(1, min(args.warmup, 2))):
+            hp.propagate_device(seeds_d.data_ptr(), n, 0, stream.cuda_stream)
+        nsl, npts = hp.counts()
+        barrier()
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        p2 = []
+        e0.record(stream)
+        for _ in range(args.steps):
+            hp.propagate_device(seeds_d.data_ptr(), n, 0, stream.cuda_stream)
+            p2.append(hp.timings()[0][2])
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        steps = float(npts - nsl)
+        if dist is not None:
+            t = torch.tensor([ms, steps], device=f"cuda:{local}", dtype=torch.float64)
+            mx = t[:1].clone()
+            dist.all_reduce(mx, op=dist.ReduceOp.MAX)
+            sm = t[1:].clone()
+            dist.all_reduce(sm)
+            ms, steps = float(mx.item()), float(sm.item())
+        return {"value": steps * args.steps / (ms / 1e3), "unit": "steps/s", "ms_per_step": ms / args.steps,
+                "pass2_ms": float(np.mean(p2)), "streamlines_per_gpu": int(nsl), "steps_per_gpu": int(npts - nsl),
+                "kernel": "track_kernel<PROB> (inverse CDF over the gathered PMF, the reference's sampler)"}
 
 
 def measured_peaks():
@@ -629,6 +678,9 @@ def main():
     ev0 = torch.cuda.Event(enable_timing=True)
     ev1 = torch.cuda.Event(enable_timing=True)
     pass2_ms, pass1_ms, compact_ms = [], [], []
+    envelope = gcfg.get("sampler") == "envelope"
+    if envelope:
+        h.sampler_stats(reset=True)
     with ClockSampler(local) as clk:
         ev0.record(stream)
         for _ in range(args.steps):
@@ -640,6 +692,7 @@ def main():
         ev1.record(stream)
         torch.cuda.synchronize()
     total_ms = ev0.elapsed_time(ev1)
+    env_stats = h.sampler_stats() if envelope else None
     barrier()
     counts = torch.tensor([float(total_ms), float(nsl), float(npts)], device=f"cuda:{local}",
                           dtype=torch.float64)
@@ -691,19 +744,33 @@ def main():
     elif model in ("CSA", "OPDT"):
         bytes_per_step = 8 * data.shape[3] * 4 + 8 * 4 + 12  # DWI corners + stop taps + point
         achieved = steps_per_batch * bytes_per_step / (p2 / 1e3) / 1e9
+    elif envelope:
+        # the sampler's algorithmic bytes: 8 corner rows of the bf16 cluster-maxima
+        # table (128 B each), the incoming direction's cone-bit row (256 B), 8 PMF
+        # values per proposal, the stop-map taps and the point write
+        props = env_stats["proposals"] / max(env_stats["steps"], 1)
+        bytes_per_step = 8 * 128 + 256 + 8 * 4 * props + 8 * 4 + 12
+        achieved = steps_per_batch * bytes_per_step / (p2 / 1e3) / 1e9
     else:
         bytes_per_step = BYTES_PER_STEP
         achieved = steps_per_batch * BYTES_PER_STEP / (p2 / 1e3) / 1e9
     traffic = None
-    if args.traffic_bytes_per_step and model == "PROB":
+    if envelope and args.env_traffic_bytes_per_step:
+        traffic = args.env_traffic_bytes_per_step * steps_per_batch
+    elif args.traffic_bytes_per_step and model == "PROB" and not envelope:
         traffic = args.traffic_bytes_per_step * steps_per_batch
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": None if achieved is None else achieved / peak, "traffic": traffic,
                 "kernel": f"track_kernel<{model}> (pass 2)",
                 "peak_source": f"{peak_kind} MEASURED_PEAKS hbm_gbs",
                 "algorithmic_bytes_per_step": bytes_per_step}
-    if model == "PROB":
+    if model == "PROB" and traffic is not None:
         roofline["traffic_source"] = "ncu dram__bytes_read+write per step at 20k seeds x steps"
+    if envelope:
+        roofline["kernel"] = "track_kernel<PROB_ENV> (pass 2, envelope sampler)"
+        # the plain kernel's algorithmic bytes per step over the same time: the
+        # rate the inverse-CDF path would need to match this kernel
+        roofline["plain_equivalent_gbs"] = steps_per_batch * BYTES_PER_STEP / (p2 / 1e3) / 1e9
     if gcfg.get("fit") == "bf16x3":
         # tensor roofline of the batched fit: algorithmic FP32-equivalent FLOP per
         # attempt (each step takes >= 1 attempt) against the measured BF16 peak;
@@ -723,6 +790,15 @@ def main():
                     "peak_source": "measured MEASURED_PEAKS bf16_tflops" if tpeak else "fallback",
                     "algorithmic_flop_per_step": flop, "issued_bf16_flop_per_step": 3 * flop}
     extra = {}
+    if envelope:
+        st = env_stats
+        extra["sampler"] = {"proposals_per_step": st["proposals"] / max(st["steps"], 1),
+                            "acceptance": st["steps"] / max(st["proposals"], 1),
+                            "exact_max_resolutions_per_step": st["resolves"] / max(st["steps"], 1),
+                            "inverse_cdf_fallbacks_per_step": st["fallbacks"] / max(st["steps"], 1)}
+    if envelope and not args.no_plain_arm:
+        extra["plain_fp32"] = plain_arm(args, data, ph, sph, gcfg, seeds_d, local, stream, barrier, dist, world)
+        extra["speedup_vs_plain_fp32"] = value / extra["plain_fp32"]["value"]
     if model == "PTT":
         frac = int(np.round(0.5 / dg.target_short_step))  # propagation sub-steps per point
         extra["sub_steps_per_s"] = value * frac

@@ -657,8 +657,10 @@ static int run_boot_batch(csl_tracker *t, const float *seeds_dev, int ni, int ns
     return CSL_OK;
 }
 
+// per_warp_fit: track boot_fit = 1 trackers with the per-warp FP32 fit (the
+// multi-subject graph's path, so an overflowed subject's re-run matches it)
 static int run_batch(csl_tracker *t, const float *seeds_dev, long long n, long long rng_base,
-                     cudaStream_t st) {
+                     cudaStream_t st, bool per_warp_fit = false) {
     const DevParams &P = t->P;
     t->ok_batch = 0;
     t->cmp_npts = -1;
@@ -699,7 +701,7 @@ static int run_batch(csl_tracker *t, const float *seeds_dev, long long n, long l
     CK(t->out_src.ensure((size_t)nsl + 1));
     CK(t->pt_off.ensure((size_t)nsl + 1));
 
-    if (t->hp.boot_fit == 1 && (P.model == CSA || P.model == OPDT)) {
+    if (t->hp.boot_fit == 1 && !per_warp_fit && (P.model == CSA || P.model == OPDT)) {
         const int r = run_boot_batch(t, seeds_dev, ni, nsl, rng_base, st);
         if (r != kUsePerWarpPath) return r;
     }
@@ -1454,7 +1456,7 @@ int csl_multi_wait(csl_multi *m, long long *n_streamlines, long long *n_points, 
         const long long *S = m->summary_h + 4 * i;
         int again = 0;
         if (m->n[i] > 0 && (S[2] & (ST_POOL_OVERFLOW | ST_SLOT_OVERFLOW))) {
-            const int rc = run_batch(u, m->seeds[i], m->n[i], m->rng_base[i], u->own_stream);
+            const int rc = run_batch(u, m->seeds[i], m->n[i], m->rng_base[i], u->own_stream, true);
             if (rc != CSL_OK) return fail(nullptr, rc, "subject %d: %s", i, u->err.c_str());
             m->sl_cap[i] = (int)std::min<long long>(
                 std::max<long long>(m->sl_cap[i], u->nsl + u->nsl / 8 + 256), (long long)INT32_MAX - 1);

@@ -187,8 +187,7 @@ __global__ void get_direction_kernel(DevParams P, const int *partner, const floa
     } else if constexpr (MODEL == PTT) {
         if (lane < 9) W.frame[lane] = frames[9 * q + lane];
         __syncwarp();
-        PttSmem S{W.face, W.vpdf};
-        ok = ptt_get_direction<false>(P, rng, d.d, W.frame, pt, S, lane, &nd.d);
+        ok = ptt_step_direction<false>(P, rng, d.d, W.frame, pt, W.face, lane, &nd.d);
         __syncwarp();
         if (lane < 9) frames[9 * q + lane] = W.frame[lane];
     } else {

@@ -86,8 +86,7 @@ __global__ void __launch_bounds__(kNoallocWarpsPerBlock * 32)
             int nB = 1, nF = 1, len = 1;
             bool single = false;
             if constexpr (MODEL == PTT) {
-                PttSmem S{W.face, W.vpdf};
-                if (!ptt_init_frame(P, rng, fs, seed, W.frame, S, lane)) single = true;
+                if (!ptt_start_frames(P, rng, fs, seed, W.frame, W.face, lane)) single = true;
             }
             if (single) {
                 if (lane == 0) store_pt(scrB, 0, seed);

@@ -85,7 +85,8 @@ struct Philox {
     }
 
     __host__ __device__ static __forceinline__ float uint_to_uniform(uint32_t x) {
-        return (float)x * 2.3283064365386963e-10f + (2.3283064365386963e-10f / 2.0f);
+        // one fused multiply-add, as the reference's fast-math build contracts it
+        return fmaf((float)x, 2.3283064365386963e-10f, 2.3283064365386963e-10f / 2.0f);
     }
 };
 

@@ -1,24 +1,51 @@
-// Parallel-transport tractography getter (ptt.cu:1-474, ptt_init.cu:5-63).
+// Parallel-transport tractography (PTT) direction getter.
 //
-// Method: Aydogan & Shi, "Parallel Transport Tractography", IEEE TMI 40(2),
-// 2021.  Each lane probes one candidate curvature (k1, k2) on a triangulated
-// disc: the frame is propagated PROBE_QUALITY times along the candidate arc
-// and the ODF amplitude is summed (the data support).  Candidates are drawn
-// from the disc-face CDF and accepted by a first-lane-above-threshold ballot.
+// Method: D. B. Aydogan and Y. Shi, "Parallel Transport Tractography", IEEE
+// TMI 40(2):635-647, 2021.  A streamline carries an orthonormal frame
+// (tangent T, normal N, binormal B).  A candidate continuation is an arc of
+// constant curvature kappa = |(k1, k2)| bending in the normal-plane direction
+// u = (k1 N + k2 B) / kappa; its data support is the ODF amplitude at the
+// current point along T plus the amplitudes at Q probe points along the arc
+// (each read along the arc's local tangent).  The sampling scheme is the one
+// the reference's get_direction_ptt_d applies (cuslines/cuda_c/ptt.cu:194-412,
+// ptt_init.cu:5-63), kept so that the output distribution is the reference's:
+//   1. supports of the 24 curvature-disc vertices (k = disc vertex * max
+//      curvature), zeroed below Q * PMF_THRESHOLD_P;
+//   2. face weights (sum of the three vertex supports, zero if any is zero)
+//      and their cumulative distribution over the 31 disc faces;
+//   3. rounds of 32 candidates drawn uniformly inside faces picked from that
+//      distribution; the first candidate (in lane order) whose support clears
+//      the threshold wins and the frame moves one step along its arc.  The
+//      initial-frame search draws a random normal per candidate and keeps the
+//      largest support.
 //
-// The ODF is read through a hardware-filtered 3D texture in the reference's
-// tiled layout (vertex t of voxel (x,y,z) at texel (tx*X+x, ty*Y+y, tz*Z+z))
-// and a point-sampled nearest-vertex LUT texture, so the filtered values are
-// the reference's own.  Normal variates use the Box-Muller transform (Box &
-// Muller 1958) on two Philox words, the second value cached for the next
-// call; the GPU tests compare them with the toolkit generator's normals
-// within a stated tolerance.
+// Design for the B200:
+//   * the frame is read from shared memory into each candidate's registers
+//     (probe frames are private to a lane); only the winner writes it back;
+//   * an arc is applied as a rotation of the frame in the (T, u) plane by
+//     theta = kappa * s:  T' = cos T + sin u,  N' = N - (k1/kappa) e,
+//     B' = B - (k2/kappa) e  with e = sin T + (1 - cos) u, and the chord
+//     d = (sin/kappa) T + ((1 - cos)/kappa) u; probe frames are not
+//     re-orthonormalised (8 rotations drift by ~1e-7), the kept frame is;
+//   * a candidate's Q probe points and tangents are computed first, then its Q
+//     nearest-vertex lookups are issued together, then its Q ODF fetches:
+//     two texture latencies per candidate instead of 2 Q dependent ones;
+//   * the face CDF is built with warp shuffles (vertex supports gathered by
+//     face, Hillis-Steele scan in registers) and searched by bisection.
 //
-// Deliberate difference: after the initial frame search the reference copies
-// only the tangent and normal into the forward half of the frame
-// (ptt.cu:464-468), leaving the forward binormal at whatever the shared slot
-// held before.  Here the forward binormal is the backward binormal, which is
-// the parallel-transported binormal the comment there describes.
+// Textures (the reference's layout, cu_direction_getters.py:531-625): the ODF
+// is hardware-filtered from a 3D texture whose vertex axis is tiled over
+// (tx, ty, tz) power-of-two tiles -- vertex t of voxel (x, y, z) sits at texel
+// (tx X + x, ty Y + y, tz Z + z) -- and directions map to vertices through a
+// point-sampled 128^3 nearest-vertex LUT addressed by (T + 1) / 2.
+//
+// Normal variates: Box-Muller (Box & Muller 1958) on two Philox words, the
+// sine value first and the cosine value cached for the next draw (the order
+// the toolkit generator's normals show, pinned by the GPU tests).
+//
+// Deliberate difference: after the initial-frame search the forward frame
+// gets the kept binormal too; the reference copies only T and N there
+// (ptt.cu:464-468) and leaves the forward binormal at a stale value.
 #pragma once
 #include "common.cuh"
 
@@ -46,10 +73,13 @@ __constant__ int c_disc_face[kDiscFaceCnt * 3] = {
     7,  10, 12, 6,  7,  3,  10, 7,  6,  3,  1,  6,  1,  5,  6,  11, 10, 6,  6,  5,  11,
     14, 19, 15, 15, 13, 14, 14, 13, 9};
 
-constexpr int kTriesPerRejection = 1024;
-constexpr float kKSmall = 0.0001f;
-constexpr float kNormEps = 1e-8f;
-constexpr float kInvNormEps = 1e8f;
+constexpr int kPttRounds = 1024 / kWarp;  // 1024 candidates at most per direction
+#ifndef CSL_PTT_WAVE
+#define CSL_PTT_WAVE 2
+#endif
+constexpr int kProbeWave = CSL_PTT_WAVE;  // probe points whose fetches are issued together
+constexpr float kCurvMin = 1e-4f;         // |k1|, |k2| below this count as straight / are raised to it
+constexpr float kTinyNorm2 = 1e-8f;
 
 // Philox with a cached second Box-Muller value (per lane).
 struct PhiloxN {
@@ -67,9 +97,6 @@ struct PhiloxN {
             has_cached = 0;
             return cached;
         }
-        // Box-Muller pair r sin(2 pi U2), r cos(2 pi U2) with r = sqrt(-2 ln U1); the
-        // sine value is returned first (the order the toolkit generator's
-        // streams show, pinned by the GPU tests)
         const float u1 = Philox::uint_to_uniform(g.next());
         const float u2 = Philox::uint_to_uniform(g.next());
         const float r = sqrtf(-2.0f * logf(u1));
@@ -81,316 +108,310 @@ struct PhiloxN {
     }
 };
 
-template <int FAIL_IND>
-__device__ __forceinline__ void norm3(float *num) {
-    const float inv_scale = rnorm3df(num[0], num[1], num[2]);
-    if (isfinite(inv_scale) && inv_scale > 0.0f && inv_scale < kInvNormEps) {
-        num[0] *= inv_scale;
-        num[1] *= inv_scale;
-        num[2] *= inv_scale;
-    } else {
-        num[0] = num[1] = num[2] = 0;
-        num[FAIL_IND] = 1.0;
-    }
-}
-
-template <int FAIL_IND>
-__device__ __forceinline__ void crossnorm3(float *dest, const float *src1, const float *src2) {
-    dest[0] = src1[1] * src2[2] - src1[2] * src2[1];
-    dest[1] = src1[2] * src2[0] - src1[0] * src2[2];
-    dest[2] = src1[0] * src2[1] - src1[1] * src2[0];
-    norm3<FAIL_IND>(dest);
-}
-
-__device__ __forceinline__ float interp4(const DevParams &P, const float3 pos, const float *frame) {
-    const float3 uvw = {fmaf(frame[0], 0.5f, 0.5f), fmaf(frame[1], 0.5f, 0.5f),
-                        fmaf(frame[2], 0.5f, 0.5f)};
-    const int odf_idx = static_cast<int>(tex3D<float>(P.lut_tex, uvw.z, uvw.y, uvw.x));
-    const int tx = odf_idx & P.width_mask;
-    const int ty = (odf_idx >> P.log2_x) & P.height_mask;
-    const int tz = (odf_idx >> (P.log2_x + P.log2_y));
-    const float x_query = (float)(tx * P.dimx) + pos.x;
-    const float y_query = (float)(ty * P.dimy) + pos.y;
-    const float z_query = (float)(tz * P.dimz) + pos.z;
-    return tex3D<float>(P.odf_tex, x_query, y_query, z_query);
-}
-
-__device__ __forceinline__ void prepare_propagator(float k1, float k2, float arclength,
-                                                   float *propagator) {
-    if ((fabsf(k1) < kKSmall) && (fabsf(k2) < kKSmall)) {
-        propagator[0] = arclength;
-        propagator[1] = 0;
-        propagator[2] = 0;
-        propagator[3] = 1;
-        propagator[4] = 0;
-        propagator[5] = 0;
-        propagator[6] = 0;
-        propagator[7] = 0;
-        propagator[8] = 1;
-    } else {
-        if (fabsf(k1) < kKSmall) k1 = kKSmall;
-        if (fabsf(k2) < kKSmall) k2 = kKSmall;
-        const float k = sqrtf(k1 * k1 + k2 * k2);
-        const float sinkt = __sinf(k * arclength);
-        const float coskt = __cosf(k * arclength);
-        const float kk = 1 / (k * k);
-        propagator[0] = sinkt / k;
-        propagator[1] = k1 * (1 - coskt) * kk;
-        propagator[2] = k2 * (1 - coskt) * kk;
-        propagator[3] = coskt;
-        propagator[4] = k1 * sinkt / k;
-        propagator[5] = k2 * sinkt / k;
-        propagator[6] = -propagator[5];
-        propagator[7] = k1 * k2 * (coskt - 1) * kk;
-        propagator[8] = (k1 * k1 + k2 * k2 * coskt) * kk;
-    }
-}
-
-__device__ __forceinline__ void random_normal(PhiloxN &st, float *probing_frame) {
-    probing_frame[3] = st.normal();
-    probing_frame[4] = st.normal();
-    probing_frame[5] = st.normal();
-    float dot = probing_frame[3] * probing_frame[0] + probing_frame[4] * probing_frame[1] +
-                probing_frame[5] * probing_frame[2];
-    probing_frame[3] -= dot * probing_frame[0];
-    probing_frame[4] -= dot * probing_frame[1];
-    probing_frame[5] -= dot * probing_frame[2];
-    float n2 = probing_frame[3] * probing_frame[3] + probing_frame[4] * probing_frame[4] +
-               probing_frame[5] * probing_frame[5];
-    if (n2 < kNormEps) {
-        float abs_x = fabsf(probing_frame[0]);
-        float abs_y = fabsf(probing_frame[1]);
-        float abs_z = fabsf(probing_frame[2]);
-        if (abs_x <= abs_y && abs_x <= abs_z) {
-            probing_frame[3] = 0.0;
-            probing_frame[4] = probing_frame[2];
-            probing_frame[5] = -probing_frame[1];
-        } else if (abs_y <= abs_z) {
-            probing_frame[3] = -probing_frame[2];
-            probing_frame[4] = 0.0;
-            probing_frame[5] = probing_frame[0];
-        } else {
-            probing_frame[3] = probing_frame[1];
-            probing_frame[4] = -probing_frame[0];
-            probing_frame[5] = 0.0;
-        }
-    }
-}
-
-template <bool IS_INIT>
-__device__ __forceinline__ void get_probing_frame(const float *frame, PhiloxN &st,
-                                                  float *probing_frame) {
-    if (IS_INIT) {
-        for (int ii = 0; ii < 3; ii++) probing_frame[ii] = frame[ii];
-        norm3<0>(probing_frame);
-        random_normal(st, probing_frame);
-        norm3<1>(probing_frame + 3);
-        crossnorm3<2>(probing_frame + 2 * 3, probing_frame, probing_frame + 3);
-    } else {
-        for (int ii = 0; ii < 9; ii++) probing_frame[ii] = frame[ii];
-    }
-}
-
-__device__ __forceinline__ void propagate_frame(const float *propagator, float *frame,
-                                                float *direc) {
-    float tmp[3];
-    for (int ii = 0; ii < 3; ii++) {
-        direc[ii] = propagator[0] * frame[ii] + propagator[1] * frame[3 + ii] +
-                    propagator[2] * frame[6 + ii];
-        tmp[ii] = propagator[3] * frame[ii] + propagator[4] * frame[3 + ii] +
-                  propagator[5] * frame[6 + ii];
-        frame[2 * 3 + ii] = propagator[6] * frame[ii] + propagator[7] * frame[3 + ii] +
-                            propagator[8] * frame[6 + ii];
-    }
-    norm3<0>(tmp);
-    crossnorm3<1>(frame + 3, frame + 2 * 3, tmp);
-    crossnorm3<2>(frame + 2 * 3, tmp, frame + 3);
-    for (int ii = 0; ii < 3; ii++) frame[ii] = tmp[ii];
-}
-
-__device__ __forceinline__ float calculate_data_support(const DevParams &P, float support,
-                                                        const float3 pos, float k1, float k2,
-                                                        float *probing_frame) {
-    float probing_prop[9];
-    float direc[3];
-    float3 probing_pos;
-    prepare_propagator(k1, k2, P.probe_step_size, probing_prop);
-    probing_pos = pos;
-    for (int ii = 0; ii < P.probe_quality; ii++) {
-        propagate_frame(probing_prop, probing_frame, direc);
-        probing_pos.x += direc[0];
-        probing_pos.y += direc[1];
-        probing_pos.z += direc[2];
-        const float fod_amp = interp4(P, probing_pos, probing_frame);
-        support += fod_amp;
-    }
-    return support;
-}
-
-struct PttSmem {
-    float *face_cdf;  // [kDiscFaceCnt]
-    float *vert_pdf;  // [kDiscVertCnt]
+struct Frame3 {
+    float3 t, n, b;
 };
 
-// get_direction_ptt_d (ptt.cu:194-412).  `frame_sh` (9 floats, shared) is the
-// warp's frame; the winning lane rewrites it.
-template <bool IS_INIT>
-__device__ int ptt_get_direction(const DevParams &P, PhiloxN &st, float3 dir, float *frame_sh,
-                                 float3 pos, const PttSmem &S, int lane, float3 *newdir) {
+__device__ __forceinline__ float3 f3_axpy(float a, float3 x, float3 y) {
+    return make_float3(fmaf(a, x.x, y.x), fmaf(a, x.y, y.y), fmaf(a, x.z, y.z));
+}
+// Products and sums are spelled out as fused or separately rounded operations
+// so that every kernel that inlines this getter rounds identically (implicit
+// contraction may differ with the surrounding code, and a PTT streamline
+// amplifies a last-bit difference into another path).
+__device__ __forceinline__ float f3_dot(float3 a, float3 b) {
+    return fmaf(a.z, b.z, fmaf(a.y, b.y, __fmul_rn(a.x, b.x)));
+}
+__device__ __forceinline__ float f3_cross_c(float p, float q, float r, float s) {
+    return fmaf(p, q, -__fmul_rn(r, s));  // p q - r s
+}
+__device__ __forceinline__ float3 f3_cross(float3 a, float3 b) {
+    return make_float3(f3_cross_c(a.y, b.z, a.z, b.y), f3_cross_c(a.z, b.x, a.x, b.z), f3_cross_c(a.x, b.y, a.y, b.x));
+}
+__device__ __forceinline__ float3 f3_scale(float a, float3 x) { return make_float3(a * x.x, a * x.y, a * x.z); }
+
+// Unit vector along v; a degenerate v (zero, huge or not finite) becomes the
+// unit axis `axis` (a measure-zero event along a streamline).
+__device__ __forceinline__ float3 unit_or_axis(float3 v, int axis) {
+    const float r = rnorm3df(v.x, v.y, v.z);
+    if (isfinite(r) && r > 0.0f && r < 1e8f) return f3_scale(r, v);
+    return make_float3(axis == 0 ? 1.0f : 0.0f, axis == 1 ? 1.0f : 0.0f, axis == 2 ? 1.0f : 0.0f);
+}
+
+// Re-orthonormalise a transported frame (tangent first, then the binormal,
+// the normal closes the right-handed triad T x N = B).
+__device__ __forceinline__ void frame_fix(Frame3 &F) {
+    F.t = unit_or_axis(F.t, 0);
+    F.b = unit_or_axis(f3_axpy(-f3_dot(F.b, F.t), F.t, F.b), 2);
+    F.n = unit_or_axis(f3_cross(F.b, F.t), 1);
+}
+
+// A circular arc of curvature (k1, k2) and length s, as a frame rotation.
+struct Arc {
+    bool straight;
+    float c, s;     // cos, sin of kappa * len
+    float kn, kb;   // k1 / kappa, k2 / kappa
+    float dt, du;   // chord = dt T + du u
+};
+
+__device__ __forceinline__ Arc make_arc(float k1, float k2, float len) {
+    Arc a;
+    a.straight = fabsf(k1) < kCurvMin && fabsf(k2) < kCurvMin;
+    if (a.straight) {
+        a.c = 1.0f;
+        a.s = a.kn = a.kb = a.du = 0.0f;
+        a.dt = len;
+        return a;
+    }
+    if (fabsf(k1) < kCurvMin) k1 = kCurvMin;
+    if (fabsf(k2) < kCurvMin) k2 = kCurvMin;
+    const float kap = sqrtf(fmaf(k1, k1, __fmul_rn(k2, k2)));
+    const float inv = 1.0f / kap;
+    __sincosf(kap * len, &a.s, &a.c);
+    a.kn = k1 * inv;
+    a.kb = k2 * inv;
+    a.dt = a.s * inv;
+    a.du = (1.0f - a.c) * inv;
+    return a;
+}
+
+// Move frame F along the arc; returns the chord (displacement).
+__device__ __forceinline__ float3 arc_move(const Arc &a, Frame3 &F) {
+    if (a.straight) return f3_scale(a.dt, F.t);
+    const float3 u = f3_axpy(a.kn, F.n, f3_scale(a.kb, F.b));
+    const float3 d = f3_axpy(a.dt, F.t, f3_scale(a.du, u));
+    const float3 e = f3_axpy(a.s, F.t, f3_scale(1.0f - a.c, u));
+    F.t = f3_axpy(a.c, F.t, f3_scale(a.s, u));
+    F.n = f3_axpy(-a.kn, e, F.n);
+    F.b = f3_axpy(-a.kb, e, F.b);
+    return d;
+}
+
+// LUT texel of a tangent, and the tiled ODF texel of a vertex at a position
+__device__ __forceinline__ float lut_vertex(const DevParams &P, float3 t) {
+    return tex3D<float>(P.lut_tex, fmaf(t.z, 0.5f, 0.5f), fmaf(t.y, 0.5f, 0.5f), fmaf(t.x, 0.5f, 0.5f));
+}
+__device__ __forceinline__ float odf_at(const DevParams &P, int v, float3 p) {
+    const int tx = v & P.width_mask;
+    const int ty = (v >> P.log2_x) & P.height_mask;
+    const int tz = v >> (P.log2_x + P.log2_y);
+    return tex3D<float>(P.odf_tex, (float)(tx * P.dimx) + p.x, (float)(ty * P.dimy) + p.y,
+                        (float)(tz * P.dimz) + p.z);
+}
+
+// Support of one candidate: `base` (the amplitude at the current point) plus
+// the amplitudes at the probe points of the arc.  F ends as the frame at the
+// last probe point.
+__device__ __forceinline__ float arc_support(const DevParams &P, float3 pos, Frame3 &F, const Arc &a, float base,
+                                             int nprobe) {
+    float sup = base;
+    for (int w0 = 0; w0 < nprobe; w0 += kProbeWave) {
+        float3 pt[kProbeWave];
+        float val[kProbeWave];
+#pragma unroll
+        for (int i = 0; i < kProbeWave; i++) {
+            if (w0 + i < nprobe) {
+                const float3 d = arc_move(a, F);
+                pos = make_float3(pos.x + d.x, pos.y + d.y, pos.z + d.z);
+                pt[i] = pos;
+                val[i] = lut_vertex(P, F.t);
+            }
+        }
+#pragma unroll
+        for (int i = 0; i < kProbeWave; i++)
+            if (w0 + i < nprobe) val[i] = odf_at(P, (int)val[i], pt[i]);
+#pragma unroll
+        for (int i = 0; i < kProbeWave; i++)
+            if (w0 + i < nprobe) sup += val[i];
+    }
+    return sup;
+}
+
+// Random frame around tangent t for the initial search: a normal drawn from
+// three Gaussian variates with the tangent component removed.
+__device__ __forceinline__ Frame3 random_frame(float3 t, PhiloxN &rng) {
+    Frame3 F;
+    F.t = unit_or_axis(t, 0);
+    float3 g;
+    g.x = rng.normal();
+    g.y = rng.normal();
+    g.z = rng.normal();
+    g = f3_axpy(-f3_dot(g, F.t), F.t, g);
+    if (f3_dot(g, g) < kTinyNorm2) {
+        // any vector orthogonal to t: drop t's smallest component
+        const float ax = fabsf(F.t.x), ay = fabsf(F.t.y), az = fabsf(F.t.z);
+        if (ax <= ay && ax <= az)
+            g = make_float3(0.0f, F.t.z, -F.t.y);
+        else if (ay <= az)
+            g = make_float3(-F.t.z, 0.0f, F.t.x);
+        else
+            g = make_float3(F.t.y, -F.t.x, 0.0f);
+    }
+    F.n = unit_or_axis(g, 1);
+    F.b = unit_or_axis(f3_cross(F.t, F.n), 2);
+    return F;
+}
+
+__device__ __forceinline__ Frame3 load_frame(const float *f) {
+    Frame3 F;
+    F.t = make_float3(f[0], f[1], f[2]);
+    F.n = make_float3(f[3], f[4], f[5]);
+    F.b = make_float3(f[6], f[7], f[8]);
+    return F;
+}
+__device__ __forceinline__ void store_frame(float *f, const Frame3 &F) {
+    f[0] = F.t.x; f[1] = F.t.y; f[2] = F.t.z;
+    f[3] = F.n.x; f[4] = F.n.y; f[5] = F.n.z;
+    f[6] = F.b.x; f[7] = F.b.y; f[8] = F.b.z;
+}
+
+// Curvature of disc vertex i (the reference scales the float table by the
+// double MAX_CURVATURE and rounds to float)
+__device__ __forceinline__ float2 disc_curv(const DevParams &P, int i) {
+    return make_float2((float)(P.max_curvature * (double)c_disc_vert[2 * i]),
+                       (float)(P.max_curvature * (double)c_disc_vert[2 * i + 1]));
+}
+
+// One PTT direction.  `frame_sh` (9 floats, shared) is the streamline's frame;
+// for INIT it receives the kept candidate's frame.  `cdf_sh` is 32 floats of
+// per-warp scratch.  Returns 0 when no candidate has enough support.
+template <bool INIT>
+__device__ int ptt_step_direction(const DevParams &P, PhiloxN &rng, float3 dir, float *frame_sh, float3 pos,
+                                  float *cdf_sh, int lane, float3 *newdir) {
+    // The frame stays in shared memory and is re-read where needed, which
+    // keeps the candidate loop's registers to one frame and one probe wave.
     __syncwarp();
-    if (IS_INIT) {
+    if (INIT) {
         if (lane == 0) {
             frame_sh[0] = dir.x;
             frame_sh[1] = dir.y;
             frame_sh[2] = dir.z;
         }
-    }
-    __syncwarp();
-    const float first_val = interp4(P, pos, frame_sh);
-    __syncwarp();
-
-    float probing_frame[9];
-    float k1_probe = 0.f, k2_probe = 0.f;
-    bool support_found = 0;
-    for (int ii = lane; ii < kDiscVertCnt; ii += kWarp) {
-        k1_probe = (float)(c_disc_vert[ii * 2] * P.max_curvature);
-        k2_probe = (float)(c_disc_vert[ii * 2 + 1] * P.max_curvature);
-        get_probing_frame<IS_INIT>(frame_sh, st, probing_frame);
-        const float this_support =
-            calculate_data_support(P, first_val, pos, k1_probe, k2_probe, probing_frame);
-        if ((double)this_support < P.probe_quality * P.pmf_threshold) {
-            S.vert_pdf[ii] = 0;
-        } else {
-            S.vert_pdf[ii] = this_support;
-            support_found = 1;
-        }
-    }
-    if (__ballot_sync(FULL, support_found) == 0) return 0;
-
-    for (int ii = lane; ii < kDiscFaceCnt; ii += kWarp) S.face_cdf[ii] = 0;
-    __syncwarp();
-    for (int ii = lane; ii < kDiscFaceCnt; ii += kWarp) {
-        for (int jj = 0; jj < 3; jj++) {
-            const float vert_val = S.vert_pdf[c_disc_face[ii * 3 + jj]];
-            if (vert_val == 0) {
-                S.face_cdf[ii] = 0;
-                break;
-            }
-            S.face_cdf[ii] += vert_val;
-        }
-    }
-    __syncwarp();
-    scan_smem_ref(S.face_cdf, kDiscFaceCnt, lane);
-    const float last_cdf = S.face_cdf[kDiscFaceCnt - 1];
-    if (last_cdf == 0) return 0;
-
-    for (int ii = 0; ii < kTriesPerRejection / kWarp; ii++) {
-        float r1 = st.uniform();
-        float r2 = st.uniform();
-        if (r1 + r2 > 1) {
-            r1 = 1 - r1;
-            r2 = 1 - r2;
-        }
-        const float tmp = st.uniform() * last_cdf;
-        int jj;
-        for (jj = 0; jj < kDiscFaceCnt - 1; jj++)
-            if (S.face_cdf[jj] >= tmp) break;
-        const double mc = P.max_curvature;
-        const float vx0 = (float)(mc * c_disc_vert[c_disc_face[jj * 3] * 2]);
-        const float vx1 = (float)(mc * c_disc_vert[c_disc_face[jj * 3 + 1] * 2]);
-        const float vx2 = (float)(mc * c_disc_vert[c_disc_face[jj * 3 + 2] * 2]);
-        const float vy0 = (float)(mc * c_disc_vert[c_disc_face[jj * 3] * 2 + 1]);
-        const float vy1 = (float)(mc * c_disc_vert[c_disc_face[jj * 3 + 1] * 2 + 1]);
-        const float vy2 = (float)(mc * c_disc_vert[c_disc_face[jj * 3 + 2] * 2 + 1]);
-        k1_probe = vx0 + r1 * (vx1 - vx0) + r2 * (vx2 - vx0);
-        k2_probe = vy0 + r1 * (vy1 - vy0) + r2 * (vy2 - vy0);
-        get_probing_frame<IS_INIT>(frame_sh, st, probing_frame);
-        const float this_support =
-            calculate_data_support(P, first_val, pos, k1_probe, k2_probe, probing_frame);
         __syncwarp();
-        int winning_lane = -1;
-        if (IS_INIT) {
-            float tmp_support = this_support;
+    }
+    const int nprobe = (int)P.probe_quality;
+    const double thr = (double)P.probe_quality * P.pmf_threshold;
+    const float3 t0 = make_float3(frame_sh[0], frame_sh[1], frame_sh[2]);
+    const float base = odf_at(P, (int)lut_vertex(P, t0), pos);
+
+    // 1. supports of the disc vertices, one per lane
+    float wv = 0.0f;
+    if (lane < kDiscVertCnt) {
+        const float2 k = disc_curv(P, lane);
+        Frame3 G = INIT ? random_frame(t0, rng) : load_frame(frame_sh);
+        const float s = arc_support(P, pos, G, make_arc(k.x, k.y, P.probe_step_size), base, nprobe);
+        wv = ((double)s < thr) ? 0.0f : s;
+    }
+    if (__ballot_sync(FULL, wv != 0.0f) == 0u) return 0;
+
+    // 2. face weights and their cumulative distribution, lane f = face f
+    const int fi = lane < kDiscFaceCnt ? lane : 0;
+    const float a = __shfl_sync(FULL, wv, c_disc_face[3 * fi]);
+    const float b = __shfl_sync(FULL, wv, c_disc_face[3 * fi + 1]);
+    const float c = __shfl_sync(FULL, wv, c_disc_face[3 * fi + 2]);
+    float cdf = (lane < kDiscFaceCnt && a != 0.0f && b != 0.0f && c != 0.0f) ? (a + b) + c : 0.0f;
 #pragma unroll
-            for (int o = 16; o > 0; o >>= 1)
-                tmp_support = fmaxf(tmp_support, __shfl_down_sync(FULL, tmp_support, o));
-            const float max_support = __shfl_sync(FULL, tmp_support, 0);
-            const unsigned msk = __ballot_sync(
-                FULL, (this_support == max_support) &&
-                          ((double)max_support >= P.probe_quality * P.pmf_threshold));
-            if (msk != 0) winning_lane = __ffs(msk) - 1;
+    for (int i = 1; i < kWarp; i <<= 1) {
+        const float y = __shfl_up_sync(FULL, cdf, i);
+        if (lane >= i) cdf += y;
+    }
+    const float total = __shfl_sync(FULL, cdf, kDiscFaceCnt - 1);
+    if (total == 0.0f) return 0;
+    cdf_sh[lane] = cdf;
+    __syncwarp();
+
+    // 3. rounds of 32 candidates
+    for (int round = 0; round < kPttRounds; round++) {
+        float r1 = rng.uniform();
+        float r2 = rng.uniform();
+        if (r1 + r2 > 1.0f) {
+            r1 = 1.0f - r1;
+            r2 = 1.0f - r2;
+        }
+        const float x = rng.uniform() * total;
+        // first face whose cumulative weight reaches x (the last face if none)
+        int lo = 0, hi = kDiscFaceCnt - 1;
+        while (lo < hi) {
+            const int mid = (lo + hi) >> 1;
+            if (cdf_sh[mid] >= x)
+                hi = mid;
+            else
+                lo = mid + 1;
+        }
+        const float2 k0 = disc_curv(P, c_disc_face[3 * lo]);
+        const float2 k1 = disc_curv(P, c_disc_face[3 * lo + 1]);
+        const float2 k2 = disc_curv(P, c_disc_face[3 * lo + 2]);
+        const float kx = fmaf(r2, k2.x - k0.x, fmaf(r1, k1.x - k0.x, k0.x));
+        const float ky = fmaf(r2, k2.y - k0.y, fmaf(r1, k1.y - k0.y, k0.y));
+        Frame3 G = INIT ? random_frame(t0, rng) : load_frame(frame_sh);
+        const float s = arc_support(P, pos, G, make_arc(kx, ky, P.probe_step_size), base, nprobe);
+        unsigned won;
+        if (INIT) {
+            const float best = warp_max_ref(s);
+            won = __ballot_sync(FULL, s == best && (double)best >= thr);
         } else {
-            const unsigned msk = __ballot_sync(
-                FULL, (double)this_support >= P.probe_quality * P.pmf_threshold);
-            if (msk != 0) winning_lane = __ffs(msk) - 1;
+            won = __ballot_sync(FULL, (double)s >= thr);
         }
-        if (winning_lane != -1) {
-            float3 nd = dir;
-            if (lane == winning_lane) {
-                if (!IS_INIT) {
-                    float prop[9];
-                    float d3[3];
-                    prepare_propagator(k1_probe, k2_probe, (float)(P.step_size / P.step_frac), prop);
-                    get_probing_frame<false>(frame_sh, st, probing_frame);
-                    propagate_frame(prop, probing_frame, d3);
-                    norm3<0>(d3);
-                    nd = make_float3(d3[0], d3[1], d3[2]);
-                }
-                for (int q = 0; q < 9; q++) frame_sh[q] = probing_frame[q];
+        if (won == 0u) continue;
+        const int src = __ffs(won) - 1;
+        float3 nd = dir;
+        __syncwarp();
+        if (lane == src) {
+            if (INIT) {
+                frame_fix(G);
+                store_frame(frame_sh, G);  // the candidate's frame at its last probe point
+            } else {
+                Frame3 H = load_frame(frame_sh);
+                const float3 d = arc_move(make_arc(kx, ky, (float)(P.step_size / P.step_frac)), H);
+                frame_fix(H);
+                store_frame(frame_sh, H);
+                nd = unit_or_axis(d, 0);
             }
-            nd.x = __shfl_sync(FULL, nd.x, winning_lane);
-            nd.y = __shfl_sync(FULL, nd.y, winning_lane);
-            nd.z = __shfl_sync(FULL, nd.z, winning_lane);
-            __syncwarp();
-            *newdir = nd;
-            return 1;
         }
+        nd.x = __shfl_sync(FULL, nd.x, src);
+        nd.y = __shfl_sync(FULL, nd.y, src);
+        nd.z = __shfl_sync(FULL, nd.z, src);
+        __syncwarp();
+        *newdir = nd;
+        return 1;
     }
     return 0;
 }
 
-// init_frame_ptt_d (ptt.cu:415-474): frame[0..8] backward, frame[9..17] forward
-__device__ __forceinline__ bool ptt_init_frame(const DevParams &P, PhiloxN &st, float3 first_step, float3 seed,
-                               float *frame, const PttSmem &S, int lane) {
-    float3 tmp;
-    bool ok = ptt_get_direction<true>(P, st, first_step, frame, seed, S, lane, &tmp);
+// Initial frames of one streamline (ptt_init.cu / init_frame_ptt_d semantics):
+// search with the pass-1 direction, else with its opposite; frame[0..8] is the
+// backward frame, frame[9..17] the forward one (T and N reversed).
+__device__ __forceinline__ bool ptt_start_frames(const DevParams &P, PhiloxN &rng, float3 first, float3 seed,
+                                                 float *frame, float *cdf_sh, int lane) {
+    float3 unused;
+    const bool fwd_ok = ptt_step_direction<true>(P, rng, first, frame, seed, cdf_sh, lane, &unused);
     __syncwarp();
-    if (!ok) {
-        ok = ptt_get_direction<true>(P, st,
-                                     make_float3(-first_step.x, -first_step.y, -first_step.z),
-                                     frame, seed, S, lane, &tmp);
-        __syncwarp();
-        if (!ok) return false;
-    } else {
-        if (lane == 0)
-            for (int ii = 0; ii < 6; ii++) frame[ii] = -frame[ii];
+    if (!fwd_ok) {
+        const float3 back = make_float3(-first.x, -first.y, -first.z);
+        if (!ptt_step_direction<true>(P, rng, back, frame, seed, cdf_sh, lane, &unused)) return false;
         __syncwarp();
     }
-    if (lane == 0) {
-        for (int ii = 0; ii < 6; ii++) frame[9 + ii] = -frame[ii];
-        for (int ii = 6; ii < 9; ii++) frame[9 + ii] = frame[ii];
+    if (lane < 9) {
+        // found along `first`: the backward frame is the reversed one
+        const float v = frame[lane];
+        const float bw = (fwd_ok && lane < 6) ? -v : v;
+        frame[lane] = bw;
+        frame[9 + lane] = (lane < 6) ? -bw : bw;
     }
     __syncwarp();
     return true;
 }
 
-// Pass-1 peaks at a seed (getNumStreamlinesPtt_k, ptt_init.cu:5-63)
-__device__ __forceinline__ int ptt_seed_peaks(const DevParams &P, float3 point, float *odf_sh,
-                                              int *ind_sh, const int *partner_sh, int lane) {
-    const int T = P.dimt;
-    for (int i = lane; i < T; i += kWarp) {
-        const int tx = i & P.width_mask;
-        const int ty = (i >> P.log2_x) & P.height_mask;
-        const int tz = (i >> (P.log2_x + P.log2_y));
-        const float xq = (float)(tx * P.dimx) + point.x;
-        const float yq = (float)(ty * P.dimy) + point.y;
-        const float zq = (float)(tz * P.dimz) + point.z;
-        float v = tex3D<float>(P.odf_tex, xq, yq, zq);
-        if ((double)v < P.pmf_threshold) v = 0.0f;
-        odf_sh[i] = v;
+// Pass 1 at a seed: ODF amplitude of every vertex from the texture,
+// thresholded, then the peak search.
+__device__ __forceinline__ int ptt_seed_odf_peaks(const DevParams &P, float3 seed, float *odf_sh, int *ind_sh,
+                                                  const int *partner_sh, int lane) {
+    for (int v = lane; v < P.dimt; v += kWarp) {
+        const float x = odf_at(P, v, seed);
+        odf_sh[v] = ((double)x < P.pmf_threshold) ? 0.0f : x;
     }
     __syncwarp();
-    return peak_directions(P, odf_sh, ind_sh, T, partner_sh, lane);
+    return peak_directions(P, odf_sh, ind_sh, P.dimt, partner_sh, lane);
 }
 
 }  // namespace csl

@@ -17,6 +17,9 @@
 #ifndef CSL_PROB_MIN_BLOCKS
 #define CSL_PROB_MIN_BLOCKS 4
 #endif
+#ifndef CSL_PTT_MIN_BLOCKS
+#define CSL_PTT_MIN_BLOCKS 2
+#endif
 
 
 namespace csl {
@@ -93,7 +96,7 @@ template <int MODEL>
 __device__ __forceinline__ int seed_peaks_dispatch(const DevParams &P, float3 seed, const WarpBufs &W,
                                    const int *partner_sh, int lane, unsigned long long subseq) {
     if (MODEL == PROB) return prob_seed_peaks(P, seed, W.odf, W.ind, partner_sh, lane);
-    if (MODEL == PTT) return ptt_seed_peaks(P, seed, W.odf, W.ind, partner_sh, lane);
+    if (MODEL == PTT) return ptt_seed_odf_peaks(P, seed, W.odf, W.ind, partner_sh, lane);
     // bootstrap: one attempt with the pass-1 stream (boot.cu:649)
     Philox rng;
     rng.init(P.rng_seed, subseq, 0);
@@ -156,8 +159,7 @@ __device__ __forceinline__ int track_one(const DevParams &P, typename RngOf<MODE
         if constexpr (MODEL == PROB) {
             ndir = prob_get_direction(P, pt, dir, W.odf, rng, lane, &nd, nullptr);
         } else if constexpr (MODEL == PTT) {
-            PttSmem S{W.face, W.vpdf};
-            ndir = ptt_get_direction<false>(P, rng, dir.d, frame, pt, S, lane, &nd.d);
+            ndir = ptt_step_direction<false>(P, rng, dir.d, frame, pt, W.face, lane, &nd.d);
         } else if constexpr (MODEL == OPDT || MODEL == CSA) {
             BootSmem S{W.vox, W.msk, W.r, W.h, W.ind};
             ndir = boot_get_direction<5, MODEL>(P, rng, dir.d, pt, S, partner_sh, lane, &nd.d,
@@ -202,7 +204,7 @@ __device__ __forceinline__ int next_seed(const BatchArgs &B) {
 
 template <int MODEL>
 __global__ void __launch_bounds__(256, base_model(MODEL) == PROB ? CSL_PROB_MIN_BLOCKS
-                                         : (MODEL == PTT ? 1 : CSL_BOOT_MIN_BLOCKS)) track_kernel(DevParams P, BatchArgs B, const int *partner,
+                                         : (MODEL == PTT ? CSL_PTT_MIN_BLOCKS : CSL_BOOT_MIN_BLOCKS)) track_kernel(DevParams P, BatchArgs B, const int *partner,
                                                     const int *__restrict__ npeaks,
                                                     const short *__restrict__ peaks, int max_store,
                                                     const int *__restrict__ sl_off, int *out_len,
@@ -255,8 +257,7 @@ __global__ void __launch_bounds__(256, base_model(MODEL) == PROB ? CSL_PROB_MIN_
                 int nB = 0, nF = 0;
                 bool single = false;
                 if constexpr (MODEL == PTT) {
-                    PttSmem S{W.face, W.vpdf};
-                    if (!ptt_init_frame(P, rng, fs, seed, W.frame, S, lane)) single = true;
+                    if (!ptt_start_frames(P, rng, fs, seed, W.frame, W.face, lane)) single = true;
                 }
                 if (single) {
                     if (lane == 0) store_pt(scrB, 0, seed);
@@ -268,8 +269,7 @@ __global__ void __launch_bounds__(256, base_model(MODEL) == PROB ? CSL_PROB_MIN_
                     DirState db{make_float3(-fs.x, -fs.y, -fs.z), pv, 1};
                     DirState df{fs, pv, 0};
                     nB = track_one<MODEL>(P, rng, seed, db, W.frame, scrB, W, partner_sh, lane, cnt);
-                    nF = track_one<MODEL>(P, rng, seed, df, W.frame + 9, scrF, W, partner_sh,
-                                                 lane, cnt);
+                    nF = track_one<MODEL>(P, rng, seed, df, W.frame + 9, scrF, W, partner_sh, lane, cnt);
                     len = nB - 1 + nF;
                 }
                 __syncwarp();

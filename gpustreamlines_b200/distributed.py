@@ -70,6 +70,38 @@ def write_shard_trx(directory: str, rank: int, counts: np.ndarray, sl_off: int, 
     offs.flush()
 
 
+def track_shard_to_trx(track, seeds: np.ndarray, rank: int, world: int, directory: str, affine,
+                       dims, global_rng_index: bool = True, group=None):
+    """One rank's whole share of a multi-GPU run into a shared TRX layout.
+
+    ``track(seeds, rng_index_base) -> (lengths, seed_index, points_vox)`` runs
+    this rank's tracker (``Handle.propagate`` + ``fetch`` on its GPU).  Seeds
+    are split contiguously (the reference's split); with ``global_rng_index``
+    seed s of the run uses the Philox streams of index s on every rank, so the
+    merged tractogram equals a one-GPU run over all seeds; without it each rank
+    restarts at index 0, which reproduces the reference's multi-GPU streams
+    (its rng offset is ignored by its kernels).  The only exchange is the
+    counts all-gather.  Rank 0 creates and seals ``directory/all.trx``.
+    """
+    import torch.distributed as dist
+
+    start, stop = shard(len(seeds), rank, world)
+    lengths, seed_idx, pts = track(seeds[start:stop], start if global_rng_index else 0)
+    counts, sl_off, pt_off = gather_counts(len(lengths), len(pts), group=group)
+    if rank == 0:
+        create_shared_trx(directory, counts)
+    dist.barrier(group)
+    aff = np.asarray(affine, dtype=np.float64)
+    world_pts = (np.asarray(pts, dtype=np.float64) @ aff[:3, :3].T + aff[:3, 3]).astype(np.float32)
+    write_shard_trx(directory, rank, counts, sl_off, pt_off, lengths, world_pts,
+                    {"DIMENSIONS": list(dims), "VOXEL_TO_RASMM": aff.tolist()})
+    dist.barrier(group)
+    if rank == 0:
+        seal_trx(directory, os.path.join(directory, "all.trx"))
+    dist.barrier(group)
+    return counts
+
+
 def create_shared_trx(directory: str, counts: np.ndarray, pos_dtype=np.float32):
     """Rank 0: allocate the shared arrays with the global sizes."""
     os.makedirs(directory, exist_ok=True)

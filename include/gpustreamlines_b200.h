@@ -209,8 +209,12 @@ int csl_philox_stream(unsigned long long seed, unsigned long long subsequence,
  *   counts_dev int32 [n]                      peaks per seed (all of them)
  *   lens_dev   int32 [n*max_peaks]            length of slot s*max_peaks+k
  *   points_dev float32 [n*max_peaks][2*max_sline_len][3]  slot s*max_peaks+k
- * Only the first min(counts[s], max_peaks) slots of a seed are written; the
- * streamlines equal csl_propagate's.  Limits (CSL_E_INVALID beyond them):
+ * Only the first min(counts[s], max_peaks) slots of a seed are written.  The
+ * kernel always runs the per-warp paths: the FP32 bootstrap fit and the
+ * inverse-CDF probabilistic sampler, so its streamlines equal csl_propagate's
+ * for trackers created with boot_fit = 0 and prob_sampler = 0 (for the other
+ * trackers they equal those of the same tracker created with 0 there).
+ * Limits (CSL_E_INVALID beyond them):
  * 1 <= max_peaks <= 32, max_sline_len <= 501, at most 1024 sphere samples.
  * The first call on a device looks up the scratch's device address (and
  * loads the module): make it before any stream capture.  All calls share
@@ -314,10 +318,12 @@ int csl_seeds_from_mask(const float *mask_dev, int X, int Y, int Z, float thresh
  * to their seed batches (device float32 [n_seeds[i], 3]; pointers and counts
  * fixed for the plan's life, contents may be rewritten between launches) and
  * runs every batch as one branch of ONE captured CUDA graph: per subject,
- * pass 1, pass 2 (the per-warp tracking path; boot_fit = 1 trackers use it
- * too) and compaction into the tracker's own result buffers, with no host
- * round trip.  Streamlines are identical to csl_propagate_device's on each
- * tracker.  Slot capacity comes from a pass-1 count at creation, pool
+ * pass 1, pass 2 (the per-warp tracking path: a boot_fit = 1 tracker is
+ * tracked with the per-warp FP32 fit, in the graph and in an overflow re-run
+ * alike) and compaction into the tracker's own result buffers, with no host
+ * round trip.  Streamlines are identical to csl_propagate_device's for
+ * trackers with boot_fit = 0 (any getter and sampler), and to those of the
+ * same tracker created with boot_fit = 0 otherwise.  Slot capacity comes from a pass-1 count at creation, pool
  * capacity from points_per_streamline (0: 128); a subject that overflows
  * either is re-run on the plain path inside csl_multi_wait (replayed[i] = 1)
  * and its capacities grow for the next launch, which re-captures the graph

@@ -36,6 +36,7 @@ class OrcParams(C.Structure):
         ("lut_res", C.c_int), ("log2_x", C.c_int), ("log2_y", C.c_int), ("tile_nx", C.c_int),
         ("tile_ny", C.c_int), ("tile_nz", C.c_int), ("step_frac", C.c_int), ("ptt_pad", C.c_int),
         ("probe_step_size", C.c_float), ("probe_quality", C.c_float), ("max_curvature", C.c_double),
+        ("rng_base", C.c_longlong),
     ]
 
 
@@ -67,7 +68,7 @@ def lib():
         L.orc_track.argtypes = [C.POINTER(OrcParams), _fp, ll, _ip, _ip, C.c_int, _ip, _ip, _fp, C.c_int]
         L.orc_track.restype = ll
         L.orc_get_direction.argtypes = [C.POINTER(OrcParams), _fp, _fp, C.POINTER(u64), C.POINTER(u64),
-                                        ll, _fp, _ip, _ip]
+                                        ll, _fp, _ip, _ip, _fp]
         L.orc_dot3_forms.argtypes = [_fp, _fp, ll, _fp]
         u32p = C.POINTER(C.c_uint32)
         L.orc_philox_block.argtypes = [u32p, u32p, u32p]
@@ -178,9 +179,11 @@ class Oracle:
                              maxp, threads)
         return counts, peaks
 
-    def track(self, seeds, threads=0, maxp=32):
-        """Full two-pass tracking -> (counts, lengths, seed index, compacted points)."""
+    def track(self, seeds, threads=0, maxp=32, rng_index_base=0):
+        """Full two-pass tracking -> (counts, lengths, seed index, compacted points).
+        Seed s uses the Philox streams of index s + rng_index_base."""
         seeds = np.ascontiguousarray(seeds, dtype=np.float32)
+        self.P.rng_base = int(rng_index_base)
         counts, peaks = self.seed_peaks(seeds, maxp, threads)
         if (counts > maxp).any():
             raise RuntimeError("oracle: raise maxp")
@@ -197,7 +200,9 @@ class Oracle:
             np.zeros((0, 3), np.float32)
         return counts, lens, sidx, flat
 
-    def get_direction(self, points, dirs, subseq, offs):
+    def get_direction(self, points, dirs, subseq, offs, frames=None):
+        """One getter call per query.  PTT takes and updates ``frames`` [n, 9]
+        (tangent, normal, binormal) and uses offset 0 of each lane's stream."""
         pts = np.ascontiguousarray(points, dtype=np.float32)
         ds = np.ascontiguousarray(dirs, dtype=np.float32)
         n = len(pts)
@@ -206,11 +211,13 @@ class Oracle:
         nd = np.zeros((n, 3), dtype=np.float32)
         ok = np.zeros(n, dtype=np.int32)
         dr = np.zeros(n, dtype=np.int32)
+        fr = None if frames is None else np.ascontiguousarray(frames, dtype=np.float32).reshape(n, 9).copy()
         lib().orc_get_direction(C.byref(self.P), _f(pts), _f(ds),
                                 sq.ctypes.data_as(C.POINTER(C.c_uint64)),
                                 of.ctypes.data_as(C.POINTER(C.c_uint64)), n, nd.ctypes.data_as(_fp),
-                                ok.ctypes.data_as(_ip), dr.ctypes.data_as(_ip))
-        return nd, ok, dr
+                                ok.ctypes.data_as(_ip), dr.ctypes.data_as(_ip),
+                                None if fr is None else fr.ctypes.data_as(_fp))
+        return (nd, ok, dr) if fr is None else (nd, ok, dr, fr)
 
     def sample_stop(self, points):
         pts = np.ascontiguousarray(points, dtype=np.float32)

@@ -51,7 +51,7 @@ def main(argv=None):
     if not available():
         print("reference sources not present; keeping prebuilt oracle/_ref")
         return 0
-    names = (argv or sys.argv[1:]) or list(CASES)
+    names = (argv or sys.argv[1:]) or [k for k, c in CASES.items() if c.get("ref", True)]
     with ThreadPoolExecutor(min(4, len(names))) as ex:
         for path in ex.map(build_case, names):
             print("built", path)

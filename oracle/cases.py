@@ -20,10 +20,10 @@ from gpustreamlines_b200.phantom import make_phantom, odf_volume, seeds_from_mas
 from gpustreamlines_b200.sphere import get_sphere
 
 CASES = {
-    # probabilistic getter on a small phantom (BASELINE config 2's parameters)
+    # probabilistic getter on a small phantom (step 0.5, 45 deg cone: the 1M-seed benchmark's parameters)
     "prob_s": dict(model="PROB", shape=(24, 28, 20), phantom_seed=7, max_angle=45.0,
                    step=0.5, fa_thr=0.1, rel=0.25, min_sep=45.0, rng_seed=0),
-    # bootstrap CSA, sh_order 6 (BASELINE config 1's parameters)
+    # bootstrap CSA, sh_order 6 (the 1000-seed bootstrap benchmark's parameters)
     "csa_s": dict(model="CSA", shape=(24, 28, 20), phantom_seed=7, max_angle=60.0, step=0.5,
                   fa_thr=0.1, rel=0.25, min_sep=45.0, rng_seed=0, sh_order=6),
     # bootstrap OPDT, sh_order 4 (the reference CLI's default model)
@@ -40,6 +40,10 @@ CASES = {
     # probabilistic getter at the full 81x106x76x724 size
     "prob_full": dict(model="PROB", shape=(81, 106, 76), phantom_seed=1234, max_angle=45.0,
                       step=0.5, fa_thr=0.1, rel=0.25, min_sep=45.0, rng_seed=0),
+    # bootstrap CSA at the full 81x106x76x160 size, sh_order 8 (the batched-fit
+    # benchmark's parameters); statistics only, so no reference library is built for it
+    "csa_full": dict(model="CSA", shape=(81, 106, 76), phantom_seed=1234, max_angle=60.0, step=0.5,
+                     fa_thr=0.1, rel=0.25, min_sep=45.0, rng_seed=0, sh_order=8, ref=False),
 }
 
 MODEL_ID = {"OPDT": 0, "CSA": 1, "PROB": 2, "PTT": 3}

@@ -77,6 +77,7 @@ typedef struct {
     int lut_res, log2_x, log2_y, tile_nx, tile_ny, tile_nz, step_frac, ptt_pad;
     float probe_step_size, probe_quality;
     double max_curvature;
+    long long rng_base;     /* Philox index of seed 0 (csl_propagate's rng_index_base) */
 } orc_params;
 
 static void set_ftz(void) {
@@ -965,7 +966,7 @@ static void ws_free(ws_t *w) {
 static int seed_peaks(const orc_params *P, const float seed[3], long long slid, ws_t *w) {
     if (P->model == PROB) return prob_seed_peaks(P, seed, w->odf, w->ind);
     if (P->model == PTT) return ptt_seed_peaks(P, seed, w->odf, w->ind);
-    for (int l = 0; l < 32; l++) philox_init(&w->lanes[l], P->rng_seed, 32ull * slid + l, 0);
+    for (int l = 0; l < 32; l++) philox_init(&w->lanes[l], P->rng_seed, 32ull * (slid + P->rng_base) + l, 0);
     float unused[3];
     const float zero[3] = {0, 0, 0};
     return boot_get_direction(P, w->lanes, 1, zero, seed, &w->bw, unused);
@@ -1049,9 +1050,9 @@ long long orc_track(const orc_params *P, const float *seeds, long long n, const 
 #endif
         for (long long s = 0; s < n; s++) {
             const float *seed = seeds + 3 * s;
-            for (int l = 0; l < 32; l++) philox_init(&w.lanes[l], P->rng_seed, 32ull * s + l + 1, 0);
+            for (int l = 0; l < 32; l++) philox_init(&w.lanes[l], P->rng_seed, 32ull * (s + P->rng_base) + l + 1, 0);
             if (P->model == PTT)
-                for (int l = 0; l < 32; l++) pttrng_init(&plane[l], P->rng_seed, 32ull * s + l + 1);
+                for (int l = 0; l < 32; l++) pttrng_init(&plane[l], P->rng_seed, 32ull * (s + P->rng_base) + l + 1);
             for (int k = 0; k < counts[s]; k++) {
                 const int pv = peaks[s * maxp + k];
                 const float *fs = P->verts + 3 * pv;
@@ -1093,7 +1094,7 @@ long long orc_track(const orc_params *P, const float *seeds, long long n, const 
 /* One direction-getter call per query (fixed position, direction, Philox
  * subsequence/offset per lane as in the device entry point). */
 int orc_get_direction(const orc_params *P, const float *pts, const float *dirs, const uint64_t *subseq,
-                      const uint64_t *offs, long long n, float *new_dirs, int *ok, int *draws) {
+                      const uint64_t *offs, long long n, float *new_dirs, int *ok, int *draws, float *frames) {
     set_ftz();
     ws_t w;
     ws_alloc(&w, P);
@@ -1102,7 +1103,12 @@ int orc_get_direction(const orc_params *P, const float *pts, const float *dirs, 
         int nd = 0;
         float out[3] = {dirs[3 * q], dirs[3 * q + 1], dirs[3 * q + 2]};
         int r;
-        if (P->model == PROB)
+        if (P->model == PTT) {
+            /* PTT generators at offset 0 of each lane's subsequence; frames[9q..9q+8] in/out */
+            pttrng_t pl[32];
+            for (int l = 0; l < 32; l++) pttrng_init(&pl[l], P->rng_seed, subseq[q] + l);
+            r = ptt_get_direction(P, pl, 0, dirs + 3 * q, frames + 9 * q, pts + 3 * q, out);
+        } else if (P->model == PROB)
             r = prob_get_direction(P, pts + 3 * q, dirs + 3 * q, w.odf, &w.lanes[0], out, &nd);
         else
             r = boot_get_direction(P, w.lanes, 5, dirs + 3 * q, pts + 3 * q, &w.bw, out);

@@ -1,8 +1,13 @@
 """Multi-rank host logic on CPU: world_size 2 with the gloo backend.
 
-Each rank fakes its shard's tracking output (no GPU); the test checks the
-contiguous seed split, the all-gather of counts and that the jointly written
-TRX equals the rank-ordered concatenation.
+Each rank tracks its contiguous seed shard with the CPU oracle (standing in
+for its GPU's tracker), all-gathers the counts and writes its slice of a
+shared TRX layout (gpustreamlines_b200.distributed.track_shard_to_trx).  The
+merged file is compared with a one-rank oracle run over all seeds:
+  * global Philox indices (each seed's streams follow its index in the whole
+    run): identical to the one-rank run, streamline for streamline;
+  * the reference's per-GPU indices (each rank restarts at 0): identical to
+    the per-shard runs concatenated in rank order.
 """
 
 from __future__ import annotations
@@ -14,6 +19,8 @@ import numpy as np
 import pytest
 import torch.multiprocessing as mp
 
+AFF = [[2.0, 0, 0, -24.0], [0, 2.0, 0, -28.0], [0, 0, 2.0, -20.0], [0, 0, 0, 1]]
+
 
 def _free_port():
     s = socket.socket()
@@ -23,57 +30,55 @@ def _free_port():
     return p
 
 
-def _fake_rank_output(rank, seeds):
-    rng = np.random.default_rng(100 + rank)
-    lens = rng.integers(1, 30, 2 * len(seeds)).astype(np.int32)
-    pts = rng.normal(size=(int(lens.sum()), 3)).astype(np.float32) + 10 * rank
-    return lens, pts
+def _oracle_track(seeds, rng_index_base):
+    from oracle import api, cases
+
+    inp = cases.inputs("prob_s")
+    _, L, S, P = api.Oracle(inp).track(seeds, threads=2, rng_index_base=rng_index_base)
+    return L, S, P
 
 
-def _worker(rank, world, port, tmp, nseeds):
+def _worker(rank, world, port, tmp, nseeds, global_index):
     import torch.distributed as dist
 
     from gpustreamlines_b200 import distributed as D
+    from oracle import cases
 
     os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
     dist.init_process_group("gloo", rank=rank, world_size=world)
     try:
-        start, stop = D.shard(nseeds, rank, world)
-        seeds = np.arange(nseeds * 3, dtype=np.float32).reshape(nseeds, 3)[start:stop]
-        lens, pts = _fake_rank_output(rank, seeds)
-        counts, sl_off, pt_off = D.gather_counts(len(lens), len(pts))
-        if rank == 0:
-            D.create_shared_trx(tmp, counts)
-        dist.barrier()
-        D.write_shard_trx(tmp, rank, counts, sl_off, pt_off, lens, pts,
-                          {"DIMENSIONS": [4, 4, 4], "VOXEL_TO_RASMM": np.eye(4).tolist()})
-        dist.barrier()
-        if rank == 0:
-            D.seal_trx(tmp, os.path.join(tmp, "all.trx"))
-        dist.barrier()
+        seeds = cases.seeds("prob_s", nseeds, seed=61)
+        D.track_shard_to_trx(_oracle_track, seeds, rank, world, tmp, AFF, cases.inputs("prob_s")["stop_map"].shape,
+                             global_rng_index=global_index)
     finally:
         dist.destroy_process_group()
 
 
-@pytest.mark.parametrize("nseeds", [7, 10])
-def test_two_rank_shards_and_trx(tmp_path, nseeds):
+def _world(P):
+    a = np.asarray(AFF)
+    return (P.astype(np.float64) @ a[:3, :3].T + a[:3, 3]).astype(np.float32)
+
+
+@pytest.mark.parametrize("global_index", [True, False])
+def test_two_rank_tracking_matches_one_rank(tmp_path, global_index):
     from gpustreamlines_b200 import distributed as D
     from gpustreamlines_b200 import io
+    from oracle import cases
 
-    world = 2
-    mp.start_processes(_worker, args=(world, _free_port(), str(tmp_path), nseeds), nprocs=world,
+    world, nseeds = 2, 301
+    mp.start_processes(_worker, args=(world, _free_port(), str(tmp_path), nseeds, global_index), nprocs=world,
                        join=True, start_method="spawn")
     hdr, seq = io.load_trx(str(tmp_path / "all.trx"))
-    want_l, want_p = [], []
-    for r in range(world):
-        a, b = D.shard(nseeds, r, world)
-        l, p = _fake_rank_output(r, np.zeros((b - a, 3)))
-        want_l.append(l)
-        want_p.append(p)
-    wl = np.concatenate(want_l)
-    assert hdr["NB_STREAMLINES"] == len(wl)
-    assert np.array_equal(seq._lengths, wl)
-    assert np.array_equal(seq._data, np.concatenate(want_p))
+    seeds = cases.seeds("prob_s", nseeds, seed=61)
+    if global_index:
+        L, _, P = _oracle_track(seeds, 0)
+    else:
+        parts = [_oracle_track(seeds[slice(*D.shard(nseeds, r, world))], 0) for r in range(world)]
+        L = np.concatenate([p[0] for p in parts])
+        P = np.concatenate([p[2] for p in parts])
+    assert hdr["NB_STREAMLINES"] == len(L) > 0
+    assert np.array_equal(np.asarray(seq._lengths), L)
+    assert np.array_equal(np.asarray(seq._data), _world(P))
 
 
 def test_shard_matches_reference_split():

@@ -333,3 +333,48 @@ def test_prob_get_direction_vs_oracle():
     assert np.array_equal(dr0, dr1)
     same = np.all(nd0 == nd1, axis=1)
     assert same.mean() == 1.0, same.mean()
+
+
+def test_ptt_step_vs_oracle():
+    """Per-step PTT directions at fixed (position, frame, per-lane Philox
+    state) against the oracle's restatement of the reference getter.  The
+    device evaluates probe arcs as frame rotations and batches its texture
+    fetches; the oracle follows the reference's propagator and emulates the
+    8-bit texture filter, so agreement is stated, not exact: the stop decision
+    agrees on >= 98 % of queries, and where both continue the new direction is
+    within 1e-3 rad on >= 97 % of queries (a near-threshold support or a draw
+    near a face boundary picks another candidate otherwise)."""
+    from oracle import api, cases
+
+    name = "ptt_s"
+    inp = cases.inputs(name)
+    h = _handle(name)
+    cos_a, cos_s = h.device_constants()
+    rng = np.random.default_rng(31)
+    n = 3000
+    pts = cases.seeds(name, n, seed=12)
+    counts, pv, _ = h.seed_peaks(pts, 4)
+    keep = counts > 0
+    pts, pv = pts[keep], pv[keep]
+    n = len(pts)
+    T = inp["vertices"][pv[:, 0]].astype(np.float64) * np.where(rng.random(n) < 0.5, -1, 1)[:, None]
+    g = rng.normal(size=(n, 3))
+    N = g - (g * T).sum(1, keepdims=True) * T
+    N /= np.linalg.norm(N, axis=1, keepdims=True)
+    B = np.cross(T, N)
+    frames = np.concatenate([T, N, B], axis=1).astype(np.float32)
+    sub = (rng.integers(0, 1 << 30, n) * 32).astype(np.uint64)
+    off = np.zeros(n, dtype=np.uint64)
+    nd0, ok0, _, fr0 = h.get_direction(pts, T.astype(np.float32), sub, off, frames=frames.copy())
+    h.close()
+    o = api.Oracle(inp, cos_max_angle=cos_a, cos_min_sep=cos_s, ptt=cases.ptt_layout(name))
+    nd1, ok1, _, fr1 = o.get_direction(pts, T.astype(np.float32), sub, off, frames=frames.copy())
+    assert (ok0 == ok1).mean() >= 0.98, (ok0 == ok1).mean()
+    both = (ok0 == 1) & (ok1 == 1)
+    assert both.sum() >= 0.5 * n
+    cosang = np.clip((nd0[both].astype(np.float64) * nd1[both]).sum(1), -1, 1)
+    close = np.arccos(cosang) < 1e-3
+    assert close.mean() >= 0.97, close.mean()
+    # the kept frame's tangent follows the same candidate
+    ct = np.clip((fr0[both, :3].astype(np.float64) * fr1[both, :3]).sum(1), -1, 1)
+    assert (np.arccos(ct)[close] < 1e-3).mean() >= 0.99
