@@ -319,12 +319,27 @@ def run_reference(args, rank, world):
     return 0
 
 
+class _DeviceArray:
+    """A DeviceBuffer seen as a CUDA array argument (used in place, not copied)."""
+
+    is_cuda = True
+
+    def __init__(self, buf):
+        self.buf = buf
+        self.shape = buf.shape
+        self.dtype = buf.dtype
+
+    def data_ptr(self):
+        return self.buf.ptr
+
+    def is_contiguous(self):
+        return True
+
+
 def run_odf_volume(args):
     """GPU ODF/PMF volume generation on the benchmark phantom (81x106x76 voxels,
     sh_order 8 -> 724 vertices, 1.9 GB written) against the host evaluation."""
-    import torch
-
-    from gpustreamlines_b200 import shm
+    from gpustreamlines_b200 import _lib, shm
     from gpustreamlines_b200.odf import odf_volume_gpu
     from gpustreamlines_b200.phantom import make_phantom
     from gpustreamlines_b200.sphere import get_sphere
@@ -333,10 +348,14 @@ def run_odf_volume(args):
     sph = get_sphere("repulsion724")
     B, _, _ = shm.real_sh_descoteaux(ph.meta["sh_order"], sph.theta, sph.phi)
     B = np.ascontiguousarray(B, dtype=np.float32)
-    coef = torch.from_numpy(np.ascontiguousarray(ph.sh_coef, dtype=np.float32)).cuda()
+    coef = _lib.DeviceBuffer.from_array(np.ascontiguousarray(ph.sh_coef, dtype=np.float32), 0)
+    dev_coef = _DeviceArray(coef)
     ms = []
+    out = None
     for i in range(args.warmup + args.steps):
-        out, m = odf_volume_gpu(coef, B, return_ms=True)
+        if out is not None:
+            out.close()
+        out, m = odf_volume_gpu(dev_coef, B, return_ms=True)
         if i >= args.warmup:
             ms.append(m)
     nvox, V, C = int(np.prod(ph.shape)), B.shape[0], B.shape[1]
@@ -349,7 +368,7 @@ def run_odf_volume(args):
     t_host = (time.perf_counter() - t0) * 8
     rows = np.nonzero(np.abs(c2).max(axis=1) > 0)[0][:: max(1, nvox // 20000)][:20000]
     ref = np.maximum(c2[rows] @ B.T, 0)
-    got = out.reshape(-1, V)[torch.from_numpy(rows).cuda()].cpu().numpy()
+    got = out.numpy().reshape(-1, V)[rows]
     err = float((np.abs(got - ref).max(axis=1) / np.maximum(np.abs(ref).max(axis=1), 1e-20)).max())
     print(json.dumps({"workload": "ODF/PMF volume from SH (81x106x76 voxels, 45 coeffs -> 724 vertices, clipped)",
                       "kernel_ms": t_kernel * 1e3, "voxels_per_s": nvox / t_kernel,
@@ -537,7 +556,7 @@ def run_learned(args):
     def track(seed, nseeds, sseed):
         ph = make_phantom((81, 106, 76), seed=seed, with_dwi=False)
         B, _, _ = shm.real_sh_descoteaux(ph.meta["sh_order"], sph.theta, sph.phi)
-        pmf = odf_volume_gpu(ph.sh_coef, B).cpu().numpy()
+        pmf = odf_volume_gpu(ph.sh_coef, B).numpy()
         seeds = seeds_from_mask(ph.fa, nseeds, threshold=0.3, seed=sseed).astype(np.float32)
         with Tracker(ProbDirectionGetter(), pmf, ph.fa, 0.1, sph.vertices, sph.edges,
                      max_angle=math.radians(45), step_size=0.5) as tr:

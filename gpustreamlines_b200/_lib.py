@@ -71,6 +71,7 @@ EXPORTS = (
     "csl_multi_create", "csl_multi_launch", "csl_multi_wait", "csl_multi_info", "csl_multi_destroy",
     "csl_multi_set_concurrency",
     "csl_set_launch", "csl_get_launch", "csl_autotune", "csl_sampler_stats", "csl_env_step",
+    "csl_device_count", "csl_dev_alloc", "csl_dev_free", "csl_dev_copy", "csl_dev_sync",
 )
 
 
@@ -130,6 +131,11 @@ def load(path: str | None = None):
     lib.csl_set_launch.argtypes = [vp, C.c_int, C.c_int]
     lib.csl_get_launch.argtypes = [vp, _ip, _ip, _ip]
     lib.csl_autotune.argtypes = [vp, vp, ll, ll, C.c_int, _fp]
+    lib.csl_device_count.argtypes = [_ip]
+    lib.csl_dev_alloc.argtypes = [C.c_int, C.c_ulonglong, C.POINTER(vp)]
+    lib.csl_dev_free.argtypes = [C.c_int, vp]
+    lib.csl_dev_copy.argtypes = [C.c_int, vp, vp, C.c_ulonglong, C.c_int]
+    lib.csl_dev_sync.argtypes = [C.c_int]
     lib.csl_sampler_stats.argtypes = [vp, ull_p, C.c_int]
     lib.csl_env_step.argtypes = [vp, _fp, _ip, _ip, ull_p, ll, _ip, _ip]
     lib.csl_last_error.argtypes = [vp, C.c_char_p, C.c_int]
@@ -184,6 +190,76 @@ def philox_stream(seed: int, subsequence: int, offset: int, n: int) -> np.ndarra
     check(lib.csl_philox_stream(seed, subsequence, offset, n,
                                 out.ctypes.data_as(C.POINTER(C.c_uint))))
     return out
+
+
+def device_count() -> int:
+    """CUDA devices visible to the library (0 without a driver or device)."""
+    n = C.c_int()
+    check(load().csl_device_count(C.byref(n)))
+    return n.value
+
+
+class DeviceBuffer:
+    """Device memory owned by the library's allocator (no framework needed).
+
+    ``DeviceBuffer(device, shape, dtype)`` allocates; ``from_array`` copies a
+    host array in; ``numpy()`` copies back; ``ptr`` is the raw device address
+    for the C ABI.  Freed on ``close()`` or garbage collection.
+    """
+
+    def __init__(self, device: int, shape, dtype=np.float32):
+        self.lib = load()
+        self.device = int(device)
+        self.shape = tuple(int(x) for x in (shape if hasattr(shape, "__len__") else (shape,)))
+        self.dtype = np.dtype(dtype)
+        self.nbytes = int(np.prod(self.shape, dtype=np.int64)) * self.dtype.itemsize
+        p = C.c_void_p()
+        check(self.lib.csl_dev_alloc(self.device, max(self.nbytes, 1), C.byref(p)))
+        self._p = p
+
+    @classmethod
+    def from_array(cls, a, device: int = 0, dtype=None):
+        a = np.ascontiguousarray(a, dtype=dtype or np.asarray(a).dtype)
+        b = cls(device, a.shape, a.dtype)
+        b.upload(a)
+        return b
+
+    @property
+    def ptr(self) -> int:
+        return self._p.value or 0
+
+    def upload(self, a):
+        a = np.ascontiguousarray(a, dtype=self.dtype)
+        if a.nbytes > self.nbytes:
+            raise ValueError("array larger than the buffer")
+        check(self.lib.csl_dev_copy(self.device, self._p, a.ctypes.data_as(C.c_void_p), a.nbytes, 1))
+
+    def numpy(self) -> np.ndarray:
+        out = np.empty(self.shape, dtype=self.dtype)
+        check(self.lib.csl_dev_copy(self.device, out.ctypes.data_as(C.c_void_p), self._p, self.nbytes, 2))
+        return out
+
+    def reshape(self, *shape):
+        shape = shape[0] if len(shape) == 1 and hasattr(shape[0], "__len__") else shape
+        if int(np.prod(shape, dtype=np.int64)) * self.dtype.itemsize != self.nbytes:
+            raise ValueError("reshape must keep the size")
+        self.shape = tuple(int(x) for x in shape)
+        return self
+
+    def close(self):
+        if getattr(self, "_p", None) is not None and self._p.value:
+            self.lib.csl_dev_free(self.device, self._p)
+        self._p = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def device_sync(device: int = 0):
+    check(load().csl_dev_sync(int(device)))
 
 
 class Handle:

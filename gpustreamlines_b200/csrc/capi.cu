@@ -1040,6 +1040,58 @@ int csl_batch_timings(csl_tracker *t, float *ms4, int *pass2_runs) {
     return CSL_OK;
 }
 
+int csl_device_count(int *n) {
+    if (!n) return fail(nullptr, CSL_E_INVALID, "n must not be NULL");
+    *n = 0;
+    const cudaError_t e = cudaGetDeviceCount(n);
+    if (e == cudaErrorNoDevice || e == cudaErrorInsufficientDriver) {
+        *n = 0;
+        cudaGetLastError();
+        return CSL_OK;
+    }
+    if (e != cudaSuccess) return fail(nullptr, CSL_E_CUDA, "cudaGetDeviceCount: %s", cudaGetErrorString(e));
+    return CSL_OK;
+}
+
+int csl_dev_alloc(int device, unsigned long long bytes, void **ptr) {
+    if (!ptr) return fail(nullptr, CSL_E_INVALID, "ptr must not be NULL");
+    *ptr = nullptr;
+    cudaError_t e = cudaSetDevice(device);
+    if (e != cudaSuccess) return fail(nullptr, CSL_E_CUDA, "cudaSetDevice(%d): %s", device, cudaGetErrorString(e));
+    e = cudaMalloc(ptr, bytes ? bytes : 1);
+    if (e != cudaSuccess) {
+        *ptr = nullptr;
+        return fail(nullptr, CSL_E_NOMEM, "cudaMalloc(%llu B): %s", bytes, cudaGetErrorString(e));
+    }
+    return CSL_OK;
+}
+
+int csl_dev_free(int device, void *ptr) {
+    if (!ptr) return CSL_OK;
+    cudaError_t e = cudaSetDevice(device);
+    if (e == cudaSuccess) e = cudaFree(ptr);
+    if (e != cudaSuccess) return fail(nullptr, CSL_E_CUDA, "cudaFree: %s", cudaGetErrorString(e));
+    return CSL_OK;
+}
+
+int csl_dev_copy(int device, void *dst, const void *src, unsigned long long bytes, int kind) {
+    if (bytes == 0) return CSL_OK;
+    if (!dst || !src || kind < 1 || kind > 3) return fail(nullptr, CSL_E_INVALID, "bad copy arguments");
+    const cudaMemcpyKind k = kind == 1 ? cudaMemcpyHostToDevice
+                                       : (kind == 2 ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice);
+    cudaError_t e = cudaSetDevice(device);
+    if (e == cudaSuccess) e = cudaMemcpy(dst, src, bytes, k);
+    if (e != cudaSuccess) return fail(nullptr, CSL_E_CUDA, "cudaMemcpy: %s", cudaGetErrorString(e));
+    return CSL_OK;
+}
+
+int csl_dev_sync(int device) {
+    cudaError_t e = cudaSetDevice(device);
+    if (e == cudaSuccess) e = cudaDeviceSynchronize();
+    if (e != cudaSuccess) return fail(nullptr, CSL_E_CUDA, "cudaDeviceSynchronize: %s", cudaGetErrorString(e));
+    return CSL_OK;
+}
+
 int csl_sampler_stats(csl_tracker *t, unsigned long long *out4, int reset) {
     if (!t) return fail(nullptr, CSL_E_INVALID, "NULL tracker");
     if (!t->P.env) return fail(t, CSL_E_STATE, "the tracker does not use the envelope sampler (prob_sampler=1)");

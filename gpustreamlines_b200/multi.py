@@ -37,8 +37,6 @@ class MultiSubjectRun:
     """
 
     def __init__(self, trackers, seeds, points_per_streamline: int = 0, rng_index_base=None):
-        import torch
-
         if len(trackers) != len(seeds) or not trackers:
             raise ValueError("one seed array per tracker, at least one tracker")
         for tr in trackers:
@@ -46,29 +44,24 @@ class MultiSubjectRun:
         self.trackers = list(trackers)
         handles = [tr.handles[0] for tr in trackers]
         device = handles[0].device
-        self._dev = torch.device("cuda", device)
         self._seeds = []
         for s in seeds:
             a = np.ascontiguousarray(np.asarray(s, dtype=np.float32).reshape(-1, 3))
-            t = torch.empty((max(len(a), 1), 3), dtype=torch.float32, device=self._dev)
+            t = _lib.DeviceBuffer(device, (max(len(a), 1), 3), np.float32)
             if len(a):
-                t[: len(a)].copy_(torch.from_numpy(a))
+                t.upload(a)
             self._seeds.append((t, len(a)))
-        torch.cuda.synchronize(self._dev)
-        self.plan = _lib.MultiPlan(handles, [t.data_ptr() for t, _ in self._seeds], [n for _, n in self._seeds],
+        self.plan = _lib.MultiPlan(handles, [t.ptr for t, _ in self._seeds], [n for _, n in self._seeds],
                                    rng_index_base, points_per_streamline)
         self.last = None
 
     def update_seeds(self, i: int, seeds):
-        import torch
-
         t, n = self._seeds[i]
         a = np.ascontiguousarray(np.asarray(seeds, dtype=np.float32).reshape(-1, 3))
         if len(a) != n:
             raise ValueError(f"subject {i}: the plan was built for {n} seeds, got {len(a)}")
         if n:
-            t[:n].copy_(torch.from_numpy(a))
-            torch.cuda.synchronize(self._dev)
+            t.upload(a)
 
     def launch(self, stream: int | None = None):
         """Launch the graph (asynchronous)."""
@@ -102,6 +95,9 @@ class MultiSubjectRun:
         if getattr(self, "plan", None) is not None:
             self.plan.close()
             self.plan = None
+        for t, _ in getattr(self, "_seeds", []):
+            t.close()
+        self._seeds = []
 
     def __enter__(self):
         return self

@@ -25,11 +25,10 @@ REAL_DTYPE = np.float32
 
 
 def device_count() -> int:
+    """CUDA devices visible (through the library; 0 when none can be used)."""
     try:
-        import torch
-
-        return torch.cuda.device_count()
-    except Exception:
+        return _lib.device_count()
+    except (RuntimeError, OSError):
         return 0
 
 
@@ -159,8 +158,6 @@ class GPUTracker(GenericTracker):
         tracking path by timing the candidates on a random sample of ``seeds``
         (``csl_autotune``).  Streamlines do not depend on the shape.  Returns,
         per GPU, {(threads_per_block, seed_order): ms or None} and the chosen shape."""
-        import torch
-
         self._allocate()
         seeds = np.ascontiguousarray(np.asarray(seeds, dtype=np.float32).reshape(-1, 3))
         if len(seeds) == 0:
@@ -169,8 +166,8 @@ class GPUTracker(GenericTracker):
         pick = seeds[rng.choice(len(seeds), size=min(sample, len(seeds)), replace=False)]
         out = []
         for h in self.handles:
-            d = torch.from_numpy(np.ascontiguousarray(pick)).to(torch.device("cuda", h.device))
-            torch.cuda.synchronize(d.device)
-            ms = h.autotune(d.data_ptr(), len(pick), 0, repeats)
+            d = _lib.DeviceBuffer.from_array(pick, h.device, np.float32)
+            ms = h.autotune(d.ptr, len(pick), 0, repeats)
+            d.close()
             out.append((ms, h.get_launch()[:2]))
         return out

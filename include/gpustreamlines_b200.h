@@ -371,6 +371,22 @@ int csl_autotune(csl_tracker *t, const float *seeds_dev, long long n, long long 
                  float *ms_out);
 
 /*
+ * Device plumbing for hosts without a CUDA runtime binding of their own (the
+ * reference's Python host uses cuda-python for these, cu_tractography.py:
+ * 189-258 and cu_propagate_seeds.py:171-204).  Synchronous.
+ *   csl_device_count  CUDA devices visible (0 without a driver or device)
+ *   csl_dev_alloc     `bytes` of device memory on `device` (*ptr = NULL on error)
+ *   csl_dev_free      release memory from csl_dev_alloc (NULL is a no-op)
+ *   csl_dev_copy      kind 1 host -> device, 2 device -> host, 3 device -> device
+ *   csl_dev_sync      wait for all work on `device`
+ */
+int csl_device_count(int *n);
+int csl_dev_alloc(int device, unsigned long long bytes, void **ptr);
+int csl_dev_free(int device, void *ptr);
+int csl_dev_copy(int device, void *dst, const void *src, unsigned long long bytes, int kind);
+int csl_dev_sync(int device);
+
+/*
  * Bounded-envelope sampler of the probabilistic getter (prob_sampler = 1; no
  * counterpart in the reference, whose sampler is the inverse CDF of
  * get_direction_prob_d, generate_streamlines_cuda.cu:54-275).

@@ -40,6 +40,9 @@ CASES = {
     # probabilistic getter at the full 81x106x76x724 size
     "prob_full": dict(model="PROB", shape=(81, 106, 76), phantom_seed=1234, max_angle=45.0,
                       step=0.5, fa_thr=0.1, rel=0.25, min_sep=45.0, rng_seed=0),
+    # PTT at the full 81x106x76 size (timing of the reference's PTT kernels)
+    "ptt_full": dict(model="PTT", shape=(81, 106, 76), phantom_seed=1234, max_angle=60.0, step=0.5,
+                     fa_thr=0.1, rel=0.25, min_sep=45.0, rng_seed=0),
     # bootstrap CSA at the full 81x106x76x160 size, sh_order 8 (the batched-fit
     # benchmark's parameters); statistics only, so no reference library is built for it
     "csa_full": dict(model="CSA", shape=(81, 106, 76), phantom_seed=1234, max_angle=60.0, step=0.5,
@@ -114,7 +117,7 @@ def macros(name):
         "REF_MODEL": str(MODEL_ID[c["model"]]),
     }
     if c["model"] == "PTT":
-        p = ptt_layout(name)
+        p = ptt_tiles(T)
         max_angle32 = np.float32(math.radians(c["max_angle"]))
         step32 = np.float32(c["step"])
         m.update({
@@ -129,6 +132,20 @@ def macros(name):
                   "MAX_CURVATURE", "PROBE_QUALITY", "STEP_FRAC"):
             m[k] = "0"
     return m
+
+
+def ptt_tiles(T):
+    """Power-of-two tile counts of the PTT texture's vertex axis (the getter's
+    prepare_data rule), without building the texture."""
+    nx = ny = nz = 1
+    while nx * ny * nz < T:
+        if nx <= ny and nx <= nz:
+            nx *= 2
+        elif ny <= nx and ny <= nz:
+            ny *= 2
+        else:
+            nz *= 2
+    return dict(nx=nx, ny=ny, nz=nz, log2_x=int(math.log2(nx)), log2_y=int(math.log2(ny)))
 
 
 @functools.lru_cache(maxsize=2)

@@ -33,7 +33,7 @@ def test_odf_volume_matches_host(clip):
     host = coef.reshape(-1, coef.shape[-1]).astype(np.float64) @ B.T.astype(np.float64)
     if clip:
         host = np.maximum(host, 0.0)
-    gpu = odf_volume_gpu(coef, B, clip=clip).cpu().numpy().reshape(host.shape)
+    gpu = odf_volume_gpu(coef, B, clip=clip).numpy().reshape(host.shape)
     scale = np.maximum(np.abs(host).max(axis=1, keepdims=True), 1e-20)
     assert (np.abs(gpu - host) / scale).max() <= 1e-4
     if clip:

@@ -23,7 +23,7 @@ def test_dti_fa_matches_float64_wls():
     gt = ph.gtab
     mask = (ph.fa > 0.05).astype(np.float32)
     ref = fp64.dti_fa_wls(ph.dwi, gt.bvals, gt.bvecs, mask=mask)
-    got = dti_fa_gpu(ph.dwi, gt.bvals, gt.bvecs, mask=mask).cpu().numpy()
+    got = dti_fa_gpu(ph.dwi, gt.bvals, gt.bvecs, mask=mask).numpy()
     assert np.abs(got - ref).max() <= 1e-6
     assert (got[mask == 0] == 0).all()
     assert got.max() > 0.5
@@ -37,7 +37,7 @@ def test_seeds_from_mask_distribution():
 
     fa = cases.phantom("prob_s").fa
     n = 200000
-    s = seeds_from_mask_gpu(fa, n, threshold=0.3, seed=7).cpu().numpy()
+    s = seeds_from_mask_gpu(fa, n, threshold=0.3, seed=7).numpy()
     v = np.floor(s + 0.5).astype(np.int64)
     assert (fa[v[:, 0], v[:, 1], v[:, 2]] > 0.3).all()
     frac = s - v
@@ -46,8 +46,8 @@ def test_seeds_from_mask_distribution():
     lin = np.ravel_multi_index(v.T, fa.shape)
     counts = np.bincount(np.searchsorted(np.ravel_multi_index(vox.T, fa.shape), lin), minlength=len(vox))
     assert chisquare(counts).pvalue > 1e-4
-    s2 = seeds_from_mask_gpu(fa, n, threshold=0.3, seed=7).cpu().numpy()
-    s3 = seeds_from_mask_gpu(fa, n, threshold=0.3, seed=8).cpu().numpy()
+    s2 = seeds_from_mask_gpu(fa, n, threshold=0.3, seed=7).numpy()
+    s3 = seeds_from_mask_gpu(fa, n, threshold=0.3, seed=8).numpy()
     assert np.array_equal(s, s2) and not np.array_equal(s, s3)
     with pytest.raises(ValueError):
         seeds_from_mask_gpu(fa, 10, threshold=2.0)
