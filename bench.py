@@ -48,8 +48,9 @@ BYTES_PER_STEP = 8 * 724 * 4 + 8 * 4 + 12  # PMF corners + stop-map taps + point
 # capture of this workload at 20,000 seeds (27.25 GB over 6,372,721 steps, see
 # profiles/track_kernel_prob_81x106x76x724.md); scaled to a full launch by steps.
 TRAFFIC_BYTES_PER_STEP = 4277.0
-# The same for track_kernel<PROB_ENV> (envelope sampler); 0 until captured.
-ENV_TRAFFIC_BYTES_PER_STEP = 0.0
+# The same for track_kernel<PROB_ENV> (envelope sampler): 6.90 GB over 6,341,719
+# steps at 20,000 seeds (profiles/track_kernel_prob_env_81x106x76x724.md).
+ENV_TRAFFIC_BYTES_PER_STEP = 1088.0
 
 
 def parse():
@@ -785,6 +786,9 @@ def main():
                 "algorithmic_bytes_per_step": bytes_per_step}
     if model == "PROB" and traffic is not None:
         roofline["traffic_source"] = "ncu dram__bytes_read+write per step at 20k seeds x steps"
+        # the HBM fraction the measured DRAM traffic implies (algorithmic bytes
+        # above include L2 hits)
+        roofline["dram_frac"] = traffic / (p2 / 1e3) / 1e9 / peak
     if envelope:
         roofline["kernel"] = "track_kernel<PROB_ENV> (pass 2, envelope sampler)"
         # the plain kernel's algorithmic bytes per step over the same time: the

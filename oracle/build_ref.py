@@ -19,7 +19,8 @@ import sys
 from concurrent.futures import ThreadPoolExecutor
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-REF_SRC = "/root/reference/cuslines/cuda_c"
+# The reference's CUDA sources: $CSL_REFERENCE_SRC, else the checkout's usual place.
+REF_SRC = os.environ.get("CSL_REFERENCE_SRC", "/root/reference/cuslines/cuda_c")
 OUT = os.path.join(HERE, "_ref")
 
 
@@ -27,11 +28,19 @@ def available() -> bool:
     return os.path.isfile(os.path.join(REF_SRC, "generate_streamlines_cuda.cu"))
 
 
+def require_sources():
+    if not available():
+        raise FileNotFoundError(
+            f"reference CUDA sources not found in {REF_SRC!r}: set CSL_REFERENCE_SRC to the directory that "
+            "holds cuslines/cuda_c/generate_streamlines_cuda.cu")
+
+
 def build_case(name: str, force: bool = False) -> str:
     from oracle.cases import macros
 
     out = os.path.join(OUT, f"ref_{name}.so")
     src = os.path.join(HERE, "ref_launcher.cu")
+    require_sources()
     if os.path.exists(out) and not force and os.path.getmtime(out) > os.path.getmtime(src):
         return out
     os.makedirs(OUT, exist_ok=True)
