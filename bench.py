@@ -767,7 +767,7 @@ def main():
     elif envelope:
         # the sampler's algorithmic bytes: 8 corner rows of the bf16 cluster-maxima
         # table (128 B each), the incoming direction's cone-bit row (256 B), 8 PMF
-        # values per proposal, the stop-map taps and the point write
+        # values per evaluated draw (4 per round), the stop-map taps and the point write
         props = env_stats["proposals"] / max(env_stats["steps"], 1)
         bytes_per_step = 8 * 128 + 256 + 8 * 4 * props + 8 * 4 + 12
         achieved = steps_per_batch * bytes_per_step / (p2 / 1e3) / 1e9
@@ -815,8 +815,8 @@ def main():
     extra = {}
     if envelope:
         st = env_stats
-        extra["sampler"] = {"proposals_per_step": st["proposals"] / max(st["steps"], 1),
-                            "acceptance": st["steps"] / max(st["proposals"], 1),
+        extra["sampler"] = {"draws_evaluated_per_step": st["proposals"] / max(st["steps"], 1),
+                            "rounds_of_4_draws_per_step": st["proposals"] / 4 / max(st["steps"], 1),
                             "exact_max_resolutions_per_step": st["resolves"] / max(st["steps"], 1),
                             "inverse_cdf_fallbacks_per_step": st["fallbacks"] / max(st["steps"], 1)}
     if envelope and not args.no_plain_arm:

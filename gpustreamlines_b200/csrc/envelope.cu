@@ -172,8 +172,9 @@ cudaError_t launch_track_env(const DevParams &P, const BatchArgs &B, const int *
 }
 
 // One envelope-sampler step per query (test entry point): query q at point
-// pts[q], incoming direction (-1)^dir_neg[q] * vertex dir_vtx[q], lane 0's
-// Philox stream at (subseq[q], offset 0).  Outputs the sampled vertex (-1 when
+// pts[q], incoming direction (-1)^dir_neg[q] * vertex dir_vtx[q]; proposals
+// from the envelope stream of subsequence 2^61 + subseq[q], the inverse-CDF
+// fallback from lane 0's stream at (subseq[q], offset 0).  Outputs the sampled vertex (-1 when
 // the getter stops) and the sign of the returned direction.
 __global__ void env_step_kernel(DevParams P, const float *pts, const int *dir_vtx, const int *dir_neg,
                                 const unsigned long long *subseq, int n, int *out_vtx, int *out_neg) {
@@ -198,7 +199,8 @@ __global__ void env_step_kernel(DevParams P, const float *pts, const int *dir_vt
     if (trilinear_vox(P, pt, vox, w)) {
         EnvLoads L;
         env_issue(P, vox, dir, lane, L);
-        ok = env_sample(P, vox, w, L, dir, W.odf, rng, lane, &nd, cnt);
+        EnvStream es{kEnvSubseqBase + subseq[q], 0ull};
+        ok = env_sample(P, vox, w, L, dir, W.odf, rng, es, lane, &nd, cnt);
     }
     if (lane == 0) {
         out_vtx[q] = ok ? nd.vtx : -1;

@@ -30,13 +30,15 @@
 // number -- the step finishes with the reference's inverse-CDF sampler on the
 // gathered rows; the sampler's output does not depend on how many proposals
 // were rejected before it, so this switch leaves the distribution unchanged.
-// Per step the sampler reads 1 KB of table, a 512 B cone-bit row and 8 x 32 B
-// sectors per proposal (about 2.3 proposals per accepted step on the 81x106x76
-// phantom) instead of 23 KB.
+// Per step the sampler reads 1 KB of table, a 256 B cone-bit row and 8 PMF
+// values per proposal (about 1.8 proposals per accepted step on the 81x106x76
+// phantom) instead of 23 KB.  Four proposals are evaluated at once, one per
+// group of 8 lanes, and taken in draw order.
 //
-// Random numbers: lane 0's Philox stream (the plain sampler's), three uniforms
-// per proposal.  Streamlines are therefore not identical to the plain path's,
-// only identically distributed.
+// Random numbers: the proposals read a Philox stream of their own per seed
+// (three uniforms per proposal); the inverse-CDF fallback draws from lane 0's
+// stream, as the plain sampler does.  Streamlines are therefore not identical
+// to the plain path's, only identically distributed.
 #pragma once
 #include "common.cuh"
 #include "kernels.h"
@@ -115,11 +117,32 @@ __device__ __forceinline__ void env_out(const DevParams &P, int v, const DirStat
     out->vtx = v;
 }
 
+// Proposal random numbers: a Philox stream of its own per seed (key
+// rng_seed, subsequence kEnvSubseqBase + global seed index), read block by
+// block: each round of kEnvGroups draws takes kEnvGroups blocks, block g
+// giving draw g its three uniforms (cluster, member, acceptance).
+constexpr unsigned long long kEnvSubseqBase = 1ull << 61;
+constexpr int kEnvGroups = 4;  // draws evaluated together, 8 lanes each
+
+struct EnvStream {
+    unsigned long long sub;   // Philox subsequence (high 64 counter bits)
+    unsigned long long nblk;  // blocks consumed (low 64 counter bits)
+};
+
+__device__ __forceinline__ uint4 env_block(const DevParams &P, const EnvStream &es, unsigned long long i) {
+    const unsigned long long lo = es.nblk + i;
+    const uint4 ctr = make_uint4((uint32_t)lo, (uint32_t)(lo >> 32), (uint32_t)es.sub, (uint32_t)(es.sub >> 32));
+    return philox4x32_10(ctr, make_uint2((uint32_t)P.rng_seed, (uint32_t)(P.rng_seed >> 32)));
+}
+
 // One direction.  `dir.vtx` must be a sphere vertex (always true along a
-// streamline: initial directions are pass-1 peaks, later ones sampled vertices).
+// streamline: initial directions are pass-1 peaks, later ones sampled
+// vertices).  Draws are made kEnvGroups at a time (lane group g = lane / 8
+// evaluates draw g) and taken in draw order, so the result is that of the
+// sequential rejection sampler.
 __device__ __forceinline__ int env_sample(const DevParams &P, const int (&vox)[8], const float (&w)[8],
                                           const EnvLoads &L, DirState dir, float *cdf_sh, PhiloxShared &rng,
-                                          int lane, DirState *out, EnvCount &cnt) {
+                                          EnvStream &es, int lane, DirState *out, EnvCount &cnt) {
     // cluster bounds U(2l), U(2l+1)
     float u0 = 0.0f, u1 = 0.0f;
 #pragma unroll
@@ -145,85 +168,92 @@ __device__ __forceinline__ int env_sample(const DevParams &P, const int (&vox)[8
     if (lane == 0) cnt.steps++;
 
     const float thr_hi = (float)(P.pmf_threshold * (double)mx_hi);
-    // proposals are made only when Z is a positive finite number
-    int t = (Z > 0.0f && Z < FLT_MAX && mx_hi > 0.0f) ? 0 : kEnvMaxTrials;
+    const int grp = lane >> 3, q = lane & 7;
+    int myvox = vox[0];
+#pragma unroll
+    for (int k = 1; k < 8; k++)
+        if (q == k) myvox = vox[k];
+    // proposals only when Z is a positive finite number
+    int round = (Z > 0.0f && Z < FLT_MAX && mx_hi > 0.0f) ? 0 : kEnvMaxTrials / kEnvGroups;
     float lo = 0.0f;         // largest P(v) evaluated: max P >= lo
     bool gathered = false;   // corner rows gathered, exact maximum known
     float m_exact = 0.0f, thr_x = 0.0f;
-    for (;;) {
-        // the draw whose acceptance waits for the exact threshold
-        int pend_v = -1;
-        float pend_pv = 0.0f;
-        for (; t < kEnvMaxTrials; t++) {
-            float a = 0.0f, b = 0.0f, g = 0.0f;
-            if (lane == 0) {
-                a = rng.uniform();
-                b = rng.uniform();
-                g = rng.uniform();
-                cnt.proposals++;
-            }
-            a = __shfl_sync(FULL, a, 0);
-            b = __shfl_sync(FULL, b, 0);
-            g = __shfl_sync(FULL, g, 0);
-            // cluster: first k whose cumulative weight reaches a * Z
-            const float x = a * Z;
+    for (; round < kEnvMaxTrials / kEnvGroups; round++) {
+        // draw g's uniforms from block g of this round (computed by lane 8g)
+        uint4 blk = make_uint4(0u, 0u, 0u, 0u);
+        if (q == 0) blk = env_block(P, es, (unsigned long long)grp);
+        es.nblk += kEnvGroups;
+        const float a = Philox::uint_to_uniform(__shfl_sync(FULL, blk.x, 0, 8));
+        const float b = Philox::uint_to_uniform(__shfl_sync(FULL, blk.y, 0, 8));
+        const float g = Philox::uint_to_uniform(__shfl_sync(FULL, blk.z, 0, 8));
+        if (lane == 0) cnt.proposals += kEnvGroups;
+        // cluster of each draw: first k whose cumulative weight reaches a * Z
+        int src = 0;
+        bool first = false;
+#pragma unroll
+        for (int d = 0; d < kEnvGroups; d++) {
+            const float x = __shfl_sync(FULL, a, 8 * d) * Z;
             const unsigned bA = __ballot_sync(FULL, c0 >= x);
             const unsigned bB = __ballot_sync(FULL, c1 >= x);
-            const int src = bB ? __ffs(bB) - 1 : kWarp - 1;
-            const bool first = (bA >> src) & 1u;
-            const float uk = __shfl_sync(FULL, first ? u0 : u1, src);
-            const unsigned mk = __shfl_sync(FULL, first ? L.cone.x : L.cone.y, src);
-            const int k = 2 * src + (first ? 0 : 1);
-            // member: uniform among the cluster's cone members
-            const int nk = __popc(mk);
-            if (nk == 0) continue;  // zero-weight cluster: not reachable, kept as a guard
-            int r = (int)(b * (float)nk);
-            if (r >= nk) r = nk - 1;
-            unsigned mm = mk;
-            for (int i = 0; i < r; i++) mm &= mm - 1u;
-            const int v = __ldg(P.env_member + k * kEnvMaxMembers + (__ffs(mm) - 1));
-            if (v < 0) continue;
-            const float pv = env_pmf_at(P, vox, w, v, lane);
-            lo = fmax_ref(lo, pv);
-            const bool take = g * uk < pv;  // accepted if p(v) = P(v)
-            if (gathered || !(pv < thr_hi) || pv < (float)(P.pmf_threshold * (double)lo)) {
-                const bool keep = gathered ? !(pv < thr_x) : !(pv < thr_hi);
-                if (keep && take) {
-                    env_out(P, v, dir, out);
-                    return 1;
-                }
-                continue;
+            const int sd = bB ? __ffs(bB) - 1 : kWarp - 1;
+            if (grp == d) {
+                src = sd;
+                first = (bA >> sd) & 1u;
             }
-            // the bracket does not decide P(v) >= thr; it matters only when
-            // the draw would be accepted
-            if (!take) continue;
-            pend_v = v;
-            pend_pv = pv;
-            break;
         }
-        if (!gathered) {
+        const float uA = __shfl_sync(FULL, u0, src), uB = __shfl_sync(FULL, u1, src);
+        const unsigned mA = __shfl_sync(FULL, L.cone.x, src), mB = __shfl_sync(FULL, L.cone.y, src);
+        const float uk = first ? uA : uB;
+        const unsigned mk = first ? mA : mB;
+        const int k = 2 * src + (first ? 0 : 1);
+        // member: uniform among the cluster's cone members
+        const int nk = __popc(mk);
+        int r = (int)(b * (float)nk);
+        if (r >= nk) r = nk - 1;
+        unsigned mm = mk;
+        for (int i = 0; i < r; i++) mm &= mm - 1u;
+        const int v = (nk > 0) ? (int)__ldg(P.env_member + k * kEnvMaxMembers + (__ffs(mm) - 1)) : -1;
+        // P(v): lane 8g+q reads corner q, the group combines in corner order
+        float dv = 0.0f;
+        if (v >= 0) dv = __ldg(P.dataf + (size_t)myvox * P.dimt + v);
+        float pv = 0.0f;
+#pragma unroll
+        for (int c = 0; c < 8; c++) pv = fma_ftz(__shfl_sync(FULL, dv, c, 8), w[c], pv);
+        lo = fmax_ref(lo, warp_max_ref(v >= 0 ? pv : 0.0f));
+        const bool take = v >= 0 && g * uk < pv;  // accepted if p(v) = P(v)
+        const bool decided = gathered || !(pv < thr_hi) || pv < (float)(P.pmf_threshold * (double)lo);
+        const bool keep = gathered ? !(pv < thr_x) : !(pv < thr_hi);
+        const unsigned acc = __ballot_sync(FULL, q == 0 && decided && keep && take);
+        const unsigned amb = __ballot_sync(FULL, q == 0 && !decided && take);
+        const unsigned ev = acc | amb;
+        if (ev == 0u) continue;
+        int win = (__ffs(ev) - 1) >> 3;
+        if ((amb >> (8 * win)) & 1u) {
+            // the first event needs the exact threshold: gather the corner rows
+            // and decide it and the draws after it in order
             m_exact = env_gather(P, vox, w, cdf_sh, lane);
             thr_x = (float)(P.pmf_threshold * (double)m_exact);
             gathered = true;
+            if (lane == 0) cnt.resolves++;
+            const unsigned acc2 = __ballot_sync(FULL, q == 0 && grp >= win && take && !(pv < thr_x));
+            if (acc2 == 0u) continue;
+            win = (__ffs(acc2) - 1) >> 3;
         }
-        if (pend_v < 0) break;  // proposals exhausted
-        if (lane == 0) cnt.resolves++;
-        if (!(pend_pv < thr_x)) {
-            env_out(P, pend_v, dir, out);
-            return 1;
-        }
-        t++;  // the pending draw is rejected: p(v) = 0
+        const int vw = __shfl_sync(FULL, v, 8 * win);
+        env_out(P, vw, dir, out);
+        return 1;
     }
     // inverse-CDF fallback on the gathered rows
     if (lane == 0) cnt.fallbacks++;
+    if (!gathered) m_exact = env_gather(P, vox, w, cdf_sh, lane);
     return prob_finish(P, m_exact, dir, cdf_sh, rng, lane, out, nullptr);
 }
 
 // tracker_d for the probabilistic getter with the envelope sampler: the loop
 // of prob_track (stop-map check of step i overlapped with the loads of step
 // i + 1), same stopping rules and point layout.
-__device__ __forceinline__ int prob_env_track(const DevParams &P, PhiloxShared &rng, float3 seed, DirState dir,
-                                              float *out, float *cdf_sh, int lane, EnvCount &cnt) {
+__device__ __forceinline__ int prob_env_track(const DevParams &P, PhiloxShared &rng, EnvStream &es, float3 seed,
+                                              DirState dir, float *out, float *cdf_sh, int lane, EnvCount &cnt) {
     float3 pt = seed;
     if (lane == 0) {
         out[0] = pt.x;
@@ -254,7 +284,7 @@ __device__ __forceinline__ int prob_env_track(const DevParams &P, PhiloxShared &
         }
         if (!inb) break;
         DirState nd;
-        if (!env_sample(P, vox, w, L, dir, cdf_sh, rng, lane, &nd, cnt)) break;
+        if (!env_sample(P, vox, w, L, dir, cdf_sh, rng, es, lane, &nd, cnt)) break;
         dir = nd;
         pt.x = (float)fma((double)dir.d.x, P.step_size, (double)pt.x);
         pt.y = (float)fma((double)dir.d.y, P.step_size, (double)pt.y);

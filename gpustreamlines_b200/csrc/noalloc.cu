@@ -63,6 +63,7 @@ __global__ void __launch_bounds__(kNoallocWarpsPerBlock * 32)
     const WarpBufs W = carve(P, smem + kMaxSortLayers * kWarp, warp, true, plist);
     const size_t slot_floats = (size_t)2 * P.max_sline_len * 3;
     EnvCount cnt = {0, 0, 0, 0};  // used only by the envelope sampler, which this kernel does not run
+    EnvStream es{0ull, 0ull};
 
     for (;;) {
         int s = 0;
@@ -93,8 +94,8 @@ __global__ void __launch_bounds__(kNoallocWarpsPerBlock * 32)
             } else {
                 DirState db{make_float3(-fs.x, -fs.y, -fs.z), pv, 1};
                 DirState df{fs, pv, 0};
-                nB = track_one<MODEL>(P, rng, seed, db, W.frame, scrB, W, partner_sh, lane, cnt);
-                nF = track_one<MODEL>(P, rng, seed, df, W.frame + 9, scrF, W, partner_sh, lane, cnt);
+                nB = track_one<MODEL>(P, rng, seed, db, W.frame, scrB, W, partner_sh, lane, cnt, es);
+                nF = track_one<MODEL>(P, rng, seed, df, W.frame + 9, scrF, W, partner_sh, lane, cnt, es);
                 len = nB - 1 + nF;
             }
             __syncwarp();

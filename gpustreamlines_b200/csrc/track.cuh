@@ -17,6 +17,9 @@
 #ifndef CSL_PROB_MIN_BLOCKS
 #define CSL_PROB_MIN_BLOCKS 4
 #endif
+#ifndef CSL_ENV_MIN_BLOCKS
+#define CSL_ENV_MIN_BLOCKS 4
+#endif
 #ifndef CSL_PTT_MIN_BLOCKS
 #define CSL_PTT_MIN_BLOCKS 2
 #endif
@@ -141,9 +144,9 @@ __device__ __forceinline__ void store_pt(float *out, int i, float3 p) {
 template <int MODEL>
 __device__ __forceinline__ int track_one(const DevParams &P, typename RngOf<MODEL>::T &rng, float3 seed,
                          DirState dir, float *frame, float *out, const WarpBufs &W,
-                         const int *partner_sh, int lane, EnvCount &cnt) {
+                         const int *partner_sh, int lane, EnvCount &cnt, EnvStream &es) {
     if constexpr (MODEL == PROB) return prob_track(P, rng, seed, dir, out, W.odf, lane);
-    if constexpr (MODEL == PROB_ENV) return prob_env_track(P, rng, seed, dir, out, W.odf, lane, cnt);
+    if constexpr (MODEL == PROB_ENV) return prob_env_track(P, rng, es, seed, dir, out, W.odf, lane, cnt);
     const int step_frac = (MODEL == PTT) ? P.step_frac : 1;
     const double ss = P.step_size / step_frac;
     float3 pt = seed;
@@ -203,7 +206,7 @@ __device__ __forceinline__ int next_seed(const BatchArgs &B) {
 }
 
 template <int MODEL>
-__global__ void __launch_bounds__(256, base_model(MODEL) == PROB ? CSL_PROB_MIN_BLOCKS
+__global__ void __launch_bounds__(256, MODEL == PROB_ENV ? CSL_ENV_MIN_BLOCKS : MODEL == PROB ? CSL_PROB_MIN_BLOCKS
                                          : (MODEL == PTT ? CSL_PTT_MIN_BLOCKS : CSL_BOOT_MIN_BLOCKS)) track_kernel(DevParams P, BatchArgs B, const int *partner,
                                                     const int *__restrict__ npeaks,
                                                     const short *__restrict__ peaks, int max_store,
@@ -249,6 +252,7 @@ __global__ void __launch_bounds__(256, base_model(MODEL) == PROB ? CSL_PROB_MIN_
         typename RngOf<MODEL>::T rng;
         if constexpr (base_model(MODEL) == PROB) rng.st = W.rng;
         rng.init(P.rng_seed, gid + 1, 0);
+        EnvStream es{kEnvSubseqBase + (unsigned long long)(s + B.rng_index_base), 0ull};
         {
             for (int k = 0; k < np; k++) {
                 const int pv = (np > max_store) ? plist[k] : (int)stored[k];
@@ -268,8 +272,8 @@ __global__ void __launch_bounds__(256, base_model(MODEL) == PROB ? CSL_PROB_MIN_
                 } else {
                     DirState db{make_float3(-fs.x, -fs.y, -fs.z), pv, 1};
                     DirState df{fs, pv, 0};
-                    nB = track_one<MODEL>(P, rng, seed, db, W.frame, scrB, W, partner_sh, lane, cnt);
-                    nF = track_one<MODEL>(P, rng, seed, df, W.frame + 9, scrF, W, partner_sh, lane, cnt);
+                    nB = track_one<MODEL>(P, rng, seed, db, W.frame, scrB, W, partner_sh, lane, cnt, es);
+                    nF = track_one<MODEL>(P, rng, seed, df, W.frame + 9, scrF, W, partner_sh, lane, cnt, es);
                     len = nB - 1 + nF;
                 }
                 __syncwarp();

@@ -390,16 +390,18 @@ int csl_dev_sync(int device);
  * Bounded-envelope sampler of the probabilistic getter (prob_sampler = 1; no
  * counterpart in the reference, whose sampler is the inverse CDF of
  * get_direction_prob_d, generate_streamlines_cuda.cu:54-275).
- *   csl_sampler_stats  out4 = {steps sampled, proposals drawn, proposals whose
- *                      threshold test needed the exact maximum (corner rows
- *                      gathered), steps finished by the inverse-CDF fallback}
+ *   csl_sampler_stats  out4 = {steps sampled, proposals evaluated (4 per round),
+ *                      rounds whose threshold test needed the exact maximum
+ *                      (corner rows gathered), steps finished by the
+ *                      inverse-CDF fallback}
  *                      accumulated over batches since creation or the last
  *                      reset (reset != 0 zeroes them after reading).
  *   csl_env_step       one direction per query with the sampler (test entry
  *                      point, like csl_get_direction): query i at points[i],
  *                      incoming direction (-1)^dir_neg[i] * vertex
- *                      dir_vertex[i], lane 0's Philox stream at
- *                      (rng_seed, subsequence[i], offset 0).  out_vertex[i] =
+ *                      dir_vertex[i]; proposals from the Philox stream
+ *                      (rng_seed, 2^61 + subsequence[i]), the inverse-CDF
+ *                      fallback from (rng_seed, subsequence[i], offset 0).  out_vertex[i] =
  *                      the sampled vertex or -1 when the getter stops;
  *                      out_neg[i] = 1 when the returned direction is its
  *                      negation.  Host arrays.
