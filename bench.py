@@ -72,6 +72,9 @@ def parse():
     ap.add_argument("--getter", default="prob_env", choices=sorted(GETTERS),
                     help="prob_env = the headline (envelope sampler, with the plain FP32 kernel timed "
                          "beside it); prob/csa/opdt/ptt/... print supplementary lines")
+    ap.add_argument("--boot-compare", action="store_true",
+                    help="bootstrap CSA sh 8 at --seeds: batched BF16x3 tensor-core fit and per-warp FP32 fit "
+                         "timed in the same run (one JSON line)")
     ap.add_argument("--no-plain-arm", action="store_true",
                     help="headline only: skip timing the plain FP32 inverse-CDF kernel beside it")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
@@ -185,6 +188,55 @@ def plain_arm(args, data, ph, sph, gcfg, seeds_d, local, stream, barrier, dist, 
                 "kernel": "track_kernel<PROB> (inverse CDF over the gathered PMF, the reference's sampler)"}
 
 
+def run_boot_compare(args):
+    """Bootstrap CSA (sh_order 8, 45 coefficients, 81x106x76x160 DWI) at --seeds:
+    the batched BF16x3 tensor-core fit and the per-warp FP32 fit (the reference's
+    arithmetic), each timed device-resident (pass 1 + pass 2 + compaction) after
+    a 10,000-seed warm-up batch, with the tensor roofline of the batched fit."""
+    from gpustreamlines_b200 import _lib, Tracker
+
+    ph, sph, data, seeds = build_workload(0, args.seeds, "csa_bf16x3")
+    d = _lib.DeviceBuffer.from_array(seeds, 0)
+    warm = _lib.DeviceBuffer.from_array(seeds[:10000], 0)
+    out = {}
+    for fit in ("bf16x3", "fp32"):
+        dg = make_getter("csa_bf16x3" if fit == "bf16x3" else "csa", ph, sph)
+        with Tracker(dg, data, ph.fa, 0.1, sph.vertices, sph.edges, max_angle=math.radians(60), step_size=0.5) as tr:
+            h = tr.handles[0]
+            h.propagate_device(warm.ptr, 10000, 0, None)
+            reps = args.steps if fit == "bf16x3" else 1
+            with ClockSampler(0) as clk:
+                t0 = time.perf_counter()
+                ms = []
+                for _ in range(reps):
+                    h.propagate_device(d.ptr, len(seeds), 0, None)
+                    (p1, gap, p2, cp), _ = h.timings()
+                    ms.append((p1 + gap + p2 + cp, p2))
+                wall = time.perf_counter() - t0
+            nsl, npts = h.counts()
+            tot = float(np.mean([m[0] for m in ms]))
+            p2 = float(np.mean([m[1] for m in ms]))
+            out[fit] = {"steps": int(npts - nsl), "streamlines": int(nsl), "batch_ms": tot, "pass2_ms": p2,
+                        "steps_per_s": (npts - nsl) / (tot / 1e3), "batches": reps, "wall_s": wall,
+                        "clocks": clk.summary()}
+            if fit == "bf16x3":
+                nc = dg.delta_nr
+                hr = int((dg.b0s_mask == 0).sum())
+                flop = 2 * 2 * hr * hr + 2 * nc * hr + 2 * nc * dg.sampling_matrix.shape[0]
+                with open(os.path.join(HERE, "MEASURED_PEAKS.json")) as f:
+                    tpeak = float(json.load(f)["bf16_tflops"])
+                tach = (npts - nsl) * flop / (p2 / 1e3) / 1e12
+                out[fit]["roofline"] = {"bound": "tensor", "achieved": tach, "peak": tpeak, "unit": "TFLOP/s",
+                                        "frac": tach / tpeak, "algorithmic_flop_per_step": flop,
+                                        "issued_bf16_flop_per_step": 3 * flop,
+                                        "peak_source": "measured MEASURED_PEAKS bf16_tflops"}
+    print(json.dumps({"workload": f"bootstrap CSA getter, sh_order 8 (45 coeffs), 81x106x76x160 DWI, {args.seeds} seeds, "
+                                  "step 0.5, max angle 60", "batched_bf16x3": out["bf16x3"], "per_warp_fp32": out["fp32"],
+                      "speedup_bf16x3_vs_fp32": out["bf16x3"]["steps_per_s"] / out["fp32"]["steps_per_s"]}),
+          flush=True)
+    return 0
+
+
 def measured_peaks():
     path = os.path.join(HERE, "MEASURED_PEAKS.json")
     if os.path.exists(path):
@@ -268,7 +320,7 @@ def cpu_baseline(ph, sph, data, seeds, seconds: float, threads: int | None = Non
         from gpustreamlines_b200.direction_getters import PttDirectionGetter
 
         pg = PttDirectionGetter()
-        tiled = pg.prepare_data(np.array(data, copy=True), inp["stop_map"], np.float32(0.1), inp["vertices"], False)
+        tiled = pg.prepare_data_host(np.array(data, copy=True), inp["stop_map"], np.float32(0.1), inp["vertices"], False)
         ptt = dict(tiled=tiled, lut=pg.sphere_vertices_lut_h, log2_x=pg.log2_x, log2_y=pg.log2_y,
                    nx=pg.nx, ny=pg.ny, nz=pg.nz, res=pg.odf_lut_res)
     ang = np.float32(_m.radians(g["max_angle"]))
@@ -642,6 +694,8 @@ def main():
         return run_multi(args) if rank == 0 else 0
     if args.impl == "reference":
         return run_reference(args, rank, world)
+    if args.boot_compare:
+        return run_boot_compare(args) if rank == 0 else 0
 
     import torch
 

@@ -72,6 +72,7 @@ EXPORTS = (
     "csl_multi_set_concurrency",
     "csl_set_launch", "csl_get_launch", "csl_autotune", "csl_sampler_stats", "csl_env_step",
     "csl_device_count", "csl_dev_alloc", "csl_dev_free", "csl_dev_copy", "csl_dev_sync",
+    "csl_ptt_layout", "csl_ptt_prepare", "csl_boot_step", "csl_boot_refit_stats",
 )
 
 
@@ -131,6 +132,11 @@ def load(path: str | None = None):
     lib.csl_set_launch.argtypes = [vp, C.c_int, C.c_int]
     lib.csl_get_launch.argtypes = [vp, _ip, _ip, _ip]
     lib.csl_autotune.argtypes = [vp, vp, ll, ll, C.c_int, _fp]
+    lib.csl_boot_step.argtypes = [vp, vp, vp, vp, ll, vp, C.c_int, vp, vp]
+    lib.csl_boot_refit_stats.argtypes = [vp, ull_p, C.c_int]
+    lib.csl_ptt_layout.argtypes = [C.c_int, _ip, _ip, _ip, _ip, _ip]
+    lib.csl_ptt_prepare.argtypes = [vp, vp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_double, vp, C.c_int, C.c_int,
+                                    C.c_int, vp, vp, vp]
     lib.csl_device_count.argtypes = [_ip]
     lib.csl_dev_alloc.argtypes = [C.c_int, C.c_ulonglong, C.POINTER(vp)]
     lib.csl_dev_free.argtypes = [C.c_int, vp]
@@ -176,6 +182,13 @@ def iptr(a: np.ndarray | None):
         return None
     assert a.dtype == np.int32 and a.flags["C_CONTIGUOUS"]
     return a.ctypes.data_as(_ip)
+
+
+def any_fptr(a):
+    """float pointer to a host numpy array or to a DeviceBuffer's device memory."""
+    if isinstance(a, DeviceBuffer):
+        return C.cast(C.c_void_p(a.ptr), _fp)
+    return fptr(a)
 
 
 def uptr(a: np.ndarray):
@@ -358,6 +371,19 @@ class Handle:
         a device buffer (fit 0: per-warp FP32, 1: batched BF16x3; see the C header)."""
         self._chk(self.lib.csl_boot_odf(self.h, C.c_void_p(points_ptr), C.c_void_p(resample_ptr), int(n),
                                         int(fit), C.c_void_p(odf_ptr), int(odf_stride), stream))
+
+    def boot_step(self, points_ptr: int, resample_ptr: int, dirs_ptr: int, n: int, odf_ptr: int, odf_stride: int,
+                  step_ptr: int, stream: int | None = None):
+        """The batched fit's step at fixed state into device buffers (see the C header)."""
+        self._chk(self.lib.csl_boot_step(self.h, C.c_void_p(points_ptr), C.c_void_p(resample_ptr),
+                                         C.c_void_p(dirs_ptr), int(n), C.c_void_p(odf_ptr), int(odf_stride),
+                                         C.c_void_p(step_ptr), stream))
+
+    def boot_refit_stats(self, reset: bool = False):
+        """{rows searched, rows fitted again in float64} of the batched fit."""
+        out = np.zeros(2, dtype=np.uint64)
+        self._chk(self.lib.csl_boot_refit_stats(self.h, uptr(out), int(bool(reset))))
+        return {"rows": int(out[0]), "refit": int(out[1])}
 
     def compress(self, affine=None, tol_error=0.1, max_segment_length=10.0, minlen=0, maxlen=None):
         """Linearise the last batch on the device in world coordinates; returns

@@ -20,7 +20,7 @@ CSRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "_csl.so")
 OBJ = os.path.join(HERE, "_build")
 SOURCES = ["kernels.cu", "boot_batch.cu", "odf_gemm.cu", "compress.cu", "mlp.cu", "dti.cu", "multi.cu",
-           "capi.cu", "noalloc.cu", "envelope.cu"]
+           "capi.cu", "noalloc.cu", "envelope.cu", "ptt_prep.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = [*ARCH, "-O3", "--use_fast_math", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC",
               "-diag-suppress", "20281"]

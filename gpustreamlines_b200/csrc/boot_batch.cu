@@ -422,6 +422,195 @@ __device__ __forceinline__ int peaks_fast(const DevParams &P, const float *odf, 
     return peaks_finish(P, odf, ind, n, partner_sh, lane);
 }
 
+// ---------------------------------------------------------------------------
+// near-tie re-evaluation in float64
+
+// True when a decision of the peak search that shapes the kept peaks lies
+// within tol x (row maximum) of flipping: the local-maximum test of a vertex
+// that could be kept, its relative-threshold test, or its order against a
+// kept peak closer than the separation angle (the descending sort decides
+// which of the two the separation filter keeps).  The BF16x3 row differs from
+// the float64 one by ~3e-5 of its maximum at most, so a row without such a
+// decision selects the float64 row's peaks.
+__device__ __forceinline__ bool near_tie(const DevParams &P, const float *odf, const int *ind, int n, int nr,
+                                         const short *__restrict__ nbr, float tol, int lane) {
+    float m = -FLT_MAX;
+    for (int v = lane; v < nr; v += kWarp) m = fmax_ref(m, odf[v]);
+    m = warp_max_ref(m);
+    if (!(m > 0.0f)) return false;
+    const float thr = (float)(P.pmf_threshold * (double)m);
+    const float tm = tol * m;
+    float mn = FLT_MAX;
+    for (int v = lane; v < nr; v += kWarp) {
+        const float x = odf[v];
+        mn = fmin_ref(mn, x < thr ? 0.0f : x);
+    }
+    float odf_min = warp_min_ref(mn);
+    odf_min = (0 > odf_min) ? 0 : odf_min;
+    const float comp = (float)(P.relative_peak_thresh * (double)(m - odf_min));
+    bool hit = false;
+    for (int v = lane; v < nr; v += kWarp) {
+        float x = odf[v];
+        x = x < thr ? 0.0f : x;
+        if (x - odf_min < comp - tm) continue;  // cannot be kept
+        bool bigger = false, close = false;
+#pragma unroll
+        for (int q = 0; q < kMaxDegree; q++) {
+            const int u = nbr[v * kMaxDegree + q];
+            if (u == v) continue;
+            float y = odf[u];
+            y = y < thr ? 0.0f : y;
+            bigger |= y > x + tm;
+            close |= fabsf(y - x) <= tm;
+        }
+        if (bigger) continue;  // not a maximum, by more than the margin
+        if (close || fabsf((x - odf_min) - comp) <= tm) {
+            hit = true;
+            continue;
+        }
+        const float3 pv = vert3(P.verts, v);
+        for (int k = 0; k < n; k++) {
+            const int p = ind[k];
+            if (p == v) continue;
+            float y = odf[p];
+            y = y < thr ? 0.0f : y;
+            if (fabsf(y - x) > tm) continue;
+            const float3 pp = vert3(P.verts, p);
+            float cs = pv.x * pp.x + pv.y * pp.y + pv.z * pp.z;
+            if (P.sphere_symm) cs = fabsf(cs);
+            if (cs > P.cos_min_sep) {
+                hit = true;
+                break;
+            }
+        }
+    }
+    return __any_sync(FULL, hit);
+}
+
+// One bootstrap attempt fitted again in float64 for a flagged row, with the
+// resample the batched fit used (the probe item's indices, or the Philox
+// words regenerated from the counters saved when they were drawn): trilinear
+// DWI in double, residual and hat products over the non-b0 volumes,
+// h + r[idx], clamp at min_signal, division by the mean clamped b0 signal, the
+// CSA transform (coefficient 0 fixed) or the OPDT form, and the sphere
+// sampling; the row is rounded to float into odf.  Arithmetic of the float64
+// accuracy reference (oracle/fp64.py).  scr: kRefitScr doubles of this warp.
+__device__ __noinline__ void boot_refit_fp64(const DevParams &P, int hr, int nblk1, const int *__restrict__ volidx,
+                                             float4 pt4, const int *pidx, const uint32_t *saved, double *scr,
+                                             float *odf, int lane) {
+    const int T = P.dimt, C = P.delta_nr, V = P.samplm_nr;
+    double *full = scr;                                        // [T]
+    double *rr = scr + 512;                                    // [hr] residuals, then the transform
+    double *hh = scr + 1024;                                   // [hr] fitted, then the bootstrap signal
+    double *cf = scr + 1536;                                   // [C]
+    int *idx = reinterpret_cast<int *>(scr + 1600);            // [hr]
+    const double px = pt4.x, py = pt4.y, pz = pt4.z;
+    const bool inb = (px >= -0.5) && (px + 0.5 < P.dimx) && (py >= -0.5) && (py + 0.5 < P.dimy) &&
+                     (pz >= -0.5) && (pz + 0.5 < P.dimz);
+    if (!inb) {
+        for (int v = lane; v < V; v += kWarp) odf[v] = 0.0f;
+        __syncwarp();
+        return;
+    }
+    // trilinear interpolation in double (corners in (i, j, k) order)
+    const double fx = floor(px), fy = floor(py), fz = floor(pz);
+    const double wx = px - fx, wy = py - fy, wz = pz - fz;
+    const int lx = fx < 0 ? 0 : (int)fx, ly = fy < 0 ? 0 : (int)fy, lz = fz < 0 ? 0 : (int)fz;
+    const int hx = min(lx + 1, P.dimx - 1), hy = min(ly + 1, P.dimy - 1), hz = min(lz + 1, P.dimz - 1);
+    for (int t = lane; t < T; t += kWarp) {
+        double acc = 0.0;
+#pragma unroll
+        for (int q = 0; q < 8; q++) {
+            const int i = q >> 2, j = (q >> 1) & 1, k = q & 1;
+            const double w = __dmul_rn(__dmul_rn(i ? wx : 1.0 - wx, j ? wy : 1.0 - wy), k ? wz : 1.0 - wz);
+            const long long vx = ((long long)(i ? hx : lx) * P.dimy + (j ? hy : ly)) * P.dimz + (k ? hz : lz);
+            acc = __dadd_rn(acc, __dmul_rn(w, (double)__ldg(P.dataf + vx * T + t)));
+        }
+        full[t] = acc;
+    }
+    __syncwarp();
+    // residual and hat products over the non-b0 volumes (volidx[0..hr))
+    for (int j = lane; j < hr; j += kWarp) {
+        double r = 0.0, h = 0.0;
+        for (int i = 0; i < hr; i++) {
+            const double s = full[volidx[i]];
+            r = fma((double)__ldg(P.R + (size_t)j * hr + i), s, r);
+            h = fma((double)__ldg(P.H + (size_t)j * hr + i), s, h);
+        }
+        rr[j] = r;
+        hh[j] = h;
+    }
+    // resample indices: given, or the batched fit's draws (part p drew columns
+    // 16b .. 16b+15 for b = p, p + 4, ... in order)
+    if (pidx) {
+        for (int j = lane; j < hr; j += kWarp) idx[j] = pidx[j];
+    } else if (lane < 4) {
+        Philox g;
+        g.key = make_uint2((uint32_t)P.rng_seed, (uint32_t)(P.rng_seed >> 32));
+        g.ctr = make_uint4(saved[5 * lane], saved[5 * lane + 1], saved[5 * lane + 2], saved[5 * lane + 3]);
+        g.out = philox4x32_10(g.ctr, g.key);
+        g.idx = (int)saved[5 * lane + 4];
+        for (int b = lane; b < nblk1; b += 4)
+            for (int e = 0; e < 16; e++)
+                if (16 * b + e < hr) idx[16 * b + e] = (int)(g.next() % (unsigned)hr);
+    }
+    __syncwarp();
+    for (int j = lane; j < hr; j += kWarp) hh[j] = hh[j] + rr[idx[j]];
+    __syncwarp();
+    for (int j = lane; j < hr; j += kWarp) full[volidx[j]] = hh[j];
+    __syncwarp();
+    // clamp, b0 mean of the clamped signal, normalise
+    const double ms = (double)P.min_signal;
+    double bs = 0.0;
+    int nb = 0;
+    for (int t = lane; t < T; t += kWarp) {
+        const double x = full[t] > ms ? full[t] : ms;
+        full[t] = x;
+        if (__ldg(P.b0s_mask + t)) {
+            bs += x;
+            nb++;
+        }
+    }
+#pragma unroll
+    for (int o = 16; o; o >>= 1) {
+        bs += __shfl_xor_sync(FULL, bs, o);
+        nb += __shfl_xor_sync(FULL, nb, o);
+    }
+    const double denom = bs / nb;
+    __syncwarp();
+    const bool opdt = P.model == OPDT;
+    for (int j = lane; j < hr; j += kWarp) {
+        const double y = full[volidx[j]] / denom;
+        hh[j] = y;
+        if (opdt) {
+            rr[j] = -log(y) * (1.5 + log(y)) * y;
+        } else {
+            const double c = y < 0.001 ? 0.001 : (y > 0.999 ? 0.999 : y);
+            rr[j] = log(-log(c));
+        }
+    }
+    __syncwarp();
+    for (int c = lane; c < C; c += kWarp) {
+        double a = 0.0;
+        for (int j = 0; j < hr; j++) a = fma((double)__ldg(P.delta_q + (size_t)c * hr + j), rr[j], a);
+        if (opdt) {
+            double b = 0.0;
+            for (int j = 0; j < hr; j++) b = fma((double)__ldg(P.delta_b + (size_t)c * hr + j), hh[j], b);
+            a -= b;
+        } else if (c == 0) {
+            a = 0.28209479177387814;  // 1 / (2 sqrt(pi))
+        }
+        cf[c] = a;
+    }
+    __syncwarp();
+    for (int v = lane; v < V; v += kWarp) {
+        double o = 0.0;
+        for (int c = 0; c < C; c++) o = fma((double)__ldg(P.sampling + (size_t)v * C + c), cf[c], o);
+        odf[v] = (float)o;
+    }
+    __syncwarp();
+}
+
 __device__ __forceinline__ void cp_async16(void *dst, const void *src) {
     asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(dst)), "l"(src) : "memory");
 }
@@ -492,6 +681,7 @@ __global__ void __launch_bounds__(kBThreads, 1)
     Philox rng;
     rng.init(0, 0, 0);
     int rng_h = -1;
+    unsigned long long rows_searched = 0, rows_refit = 0;  // lane-uniform per warp
 
     for (;;) {
         // ---- refill empty slots from the queue of streamline halves
@@ -503,6 +693,8 @@ __global__ void __launch_bounds__(kBThreads, 1)
                 } else {
                     my_h = h;
                     my_pt = make_float3(A.probe_pts[3 * h], A.probe_pts[3 * h + 1], A.probe_pts[3 * h + 2]);
+                    if (A.probe_dirs)
+                        my_dir = make_float3(A.probe_dirs[3 * h], A.probe_dirs[3 * h + 1], A.probe_dirs[3 * h + 2]);
                     my_i = 1;
                 }
             } else if (my_h < 0 && !queue_empty) {
@@ -668,6 +860,14 @@ __global__ void __launch_bounds__(kBThreads, 1)
                 rng.init(P.rng_seed,
                          kBatchSubseqBase + 8ull * (unsigned long long)(sl + A.rng_base) + 4 * half + part, 0);
                 rng_h = h;
+            }
+            if (live && !pidx && A.refit) {
+                uint32_t *sv = A.rng_save + (((size_t)blockIdx.x * kSlots + eslot) * 4 + part) * 5;
+                sv[0] = rng.ctr.x;
+                sv[1] = rng.ctr.y;
+                sv[2] = rng.ctr.z;
+                sv[3] = rng.ctr.w;
+                sv[4] = (uint32_t)rng.idx;
             }
             const bool opdt = P.model == OPDT;
             for (int b = part; b < nblk1; b += 4) {
@@ -848,7 +1048,7 @@ __global__ void __launch_bounds__(kBThreads, 1)
             __syncthreads();
         }
 
-        if (A.nprobe > 0) {  // probe mode: the ODF rows are the output
+        if (A.nprobe > 0 && !A.probe_dirs) {  // probe mode: the ODF rows are the output
             if (t < kSlots) my_h = -1;
             continue;
         }
@@ -863,7 +1063,8 @@ __global__ void __launch_bounds__(kBThreads, 1)
             for (int i = 0; i < kSlots / kBWarps; i++) live |= (s_live[base + i] ? 1u : 0u) << i;
             const int nch = g.vstride / 4;
             auto fetch = [&](int slot, float *dst) {
-                const float *src = A.odf + ((size_t)blockIdx.x * kSlots + slot) * g.vstride;
+                const float *src = A.nprobe > 0 ? A.probe_odf + (size_t)s_h[slot] * A.probe_stride
+                                                : A.odf + ((size_t)blockIdx.x * kSlots + slot) * g.vstride;
                 for (int c = lane; c < nch; c += kWarp) cp_async16(dst + 4 * c, src + 4 * c);
             };
             int cur = live ? __ffs(live) - 1 : -1;
@@ -879,12 +1080,27 @@ __global__ void __launch_bounds__(kBThreads, 1)
                 __syncwarp();
                 float *odf_sh = obuf + buf * g.vstride;
                 const int slot = base + cur;
-                int ndir = peaks_fast(P, odf_sh, ind_sh, g.V, nbr_sh, partner_sh, lane);
-                if (ndir < 0) {
-                    float m = -FLT_MAX;
-                    for (int v = lane; v < g.V; v += kWarp) m = fmax_ref(m, odf_sh[v]);
-                    m = warp_max_ref(m);
-                    ndir = peaks_sparse(P, odf_sh, ind_sh, g.V, m, nbr_sh, partner_sh, lane);
+                int ndir = -1;
+                bool refitted = false;
+                for (int pass = 0; pass < 2; pass++) {
+                    ndir = peaks_fast(P, odf_sh, ind_sh, g.V, nbr_sh, partner_sh, lane);
+                    if (ndir < 0) {
+                        float m = -FLT_MAX;
+                        for (int v = lane; v < g.V; v += kWarp) m = fmax_ref(m, odf_sh[v]);
+                        m = warp_max_ref(m);
+                        ndir = peaks_sparse(P, odf_sh, ind_sh, g.V, m, nbr_sh, partner_sh, lane);
+                    }
+                    if (pass == 1 || !A.refit) break;
+                    rows_searched++;
+                    if (!near_tie(P, odf_sh, ind_sh, ndir, g.V, nbr_sh, A.refit_tol, lane)) break;
+                    // the decision is within the BF16x3 error: fit this row again in float64
+                    const int h = s_h[slot];
+                    boot_refit_fp64(P, g.hr, g.HP / 16, A.volidx, s_pt[slot],
+                                    A.nprobe > 0 ? A.probe_idx + (size_t)h * g.hr : nullptr,
+                                    A.rng_save + ((size_t)blockIdx.x * kSlots + slot) * 20,
+                                    A.refit_scr + ((size_t)blockIdx.x * kBWarps + w) * kRefitScr, odf_sh, lane);
+                    refitted = true;
+                    rows_refit++;
                 }
                 int found = 0;
                 float3 pk = make_float3(0, 0, 0);
@@ -893,13 +1109,22 @@ __global__ void __launch_bounds__(kBThreads, 1)
                     found = closest_peak(P, make_float3(d4.x, d4.y, d4.z), ndir, ind_sh, lane, &pk);
                 }
                 __syncwarp();
-                if (lane == 0) s_new[slot] = make_float4(pk.x, pk.y, pk.z, found ? 1.0f : 0.0f);
+                if (lane == 0) {
+                    s_new[slot] = make_float4(pk.x, pk.y, pk.z, found ? 1.0f : 0.0f);
+                    if (A.nprobe > 0)
+                        reinterpret_cast<float4 *>(A.probe_step)[s_h[slot]] =
+                            make_float4(pk.x, pk.y, pk.z, (found ? 1.0f : 0.0f) + (refitted ? 2.0f : 0.0f));
+                }
                 cur = nxt;
                 buf ^= 1;
             }
             asm volatile("cp.async.wait_all;" ::: "memory");
         }
         __syncthreads();
+        if (A.nprobe > 0) {  // probe mode with directions: one search per item
+            if (t < kSlots) my_h = -1;
+            continue;
+        }
 
         // ---- step (tracker_boot_d, boot.cu:725-824): one attempt per iteration
         if (w < kSlots / kWarp) {
@@ -959,6 +1184,10 @@ __global__ void __launch_bounds__(kBThreads, 1)
         }
     }
 
+    if (A.refit && A.refit_count && lane == 0 && rows_searched) {
+        atomicAdd(A.refit_count, rows_searched);
+        atomicAdd(A.refit_count + 1, rows_refit);
+    }
     // ---- teardown: every MMA has completed (each batch was waited for)
     tc_fence_before();
     __syncthreads();

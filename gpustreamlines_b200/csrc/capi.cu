@@ -89,6 +89,9 @@ struct csl_tracker {
     DevBuf<short> bb_sl_vert;
     DevBuf<long long> bb_half_off;
     DevBuf<float> bb_odf, bb_pts, bb_dwi;
+    DevBuf<uint32_t> bb_rng_save;                 // near-tie re-evaluation: saved Philox counters
+    DevBuf<double> bb_refit_scr;                  // float64 scratch, per warp
+    DevBuf<unsigned long long> bb_refit_count;    // rows searched, rows fitted again
     // compression of the last batch (csl_compress)
     DevBuf<float> cmp_world, cmp_pts;
     DevBuf<unsigned char> cmp_keep;
@@ -115,7 +118,10 @@ int tracker_view(csl_tracker *t, DevParams *P, const int **partner, int *device)
     return CSL_OK;
 }
 int tracker_fail(csl_tracker *t, int code, const char *msg) {
-    if (t) t->err = msg;
+    if (t)
+        t->err = msg;
+    else
+        g_lib_error = msg;
     return code;
 }
 }  // namespace csl
@@ -185,16 +191,16 @@ static std::vector<int> merge_exchange_partners() {
     return flat;
 }
 
-static int make_texture3d(csl_tracker *t, const float *host, int w, int h, int d, bool border,
+static int make_texture3d(csl_tracker *t, const float *src, int w, int h, int d, bool border,
                           bool linear, bool normalized, cudaArray_t *arr, cudaTextureObject_t *tex) {
     cudaChannelFormatDesc cd = cudaCreateChannelDesc(32, 0, 0, 0, cudaChannelFormatKindFloat);
     cudaExtent ext = make_cudaExtent(w, h, d);
     CK(cudaMalloc3DArray(arr, &cd, ext, 0));
     cudaMemcpy3DParms cp = {};
-    cp.srcPtr = make_cudaPitchedPtr((void *)host, (size_t)w * 4, w, h);
+    cp.srcPtr = make_cudaPitchedPtr((void *)src, (size_t)w * 4, w, h);
     cp.dstArray = *arr;
     cp.extent = ext;
-    cp.kind = cudaMemcpyHostToDevice;
+    cp.kind = cudaMemcpyDefault;  // host or device source (unified addressing)
     CK(cudaMemcpy3D(&cp));
     cudaResourceDesc rd = {};
     rd.resType = cudaResourceTypeArray;
@@ -258,6 +264,9 @@ static void release_all(csl_tracker *t) {
     t->bb_odf.release();
     t->bb_pts.release();
     t->bb_dwi.release();
+    t->bb_rng_save.release();
+    t->bb_refit_scr.release();
+    t->bb_refit_count.release();
     t->cmp_world.release();
     t->cmp_pts.release();
     t->cmp_keep.release();
@@ -302,8 +311,9 @@ static int validate(const csl_params *p, const csl_inputs *in, csl_tracker *t) {
         if (p->samplm_nr != p->nvertices)
             return fail(t, CSL_E_INVALID, "sampling_matrix rows (%d) must equal sphere vertices (%d)",
                         p->samplm_nr, p->nvertices);
-        if (p->boot_fit != 0 && p->boot_fit != 1) return fail(t, CSL_E_INVALID, "boot_fit must be 0 or 1");
-        if (p->boot_fit == 1) {
+        if (p->boot_fit < 0 || p->boot_fit > 2) return fail(t, CSL_E_INVALID, "boot_fit must be 0, 1 or 2");
+        if (p->boot_fit >= 1) {
+            if (p->dimt > 512) return fail(t, CSL_E_INVALID, "boot_fit=1 supports at most 512 volumes");
             if (p->delta_nr > 64) return fail(t, CSL_E_INVALID, "boot_fit=1 supports at most 64 SH coefficients");
             if (p->samplm_nr > 768) return fail(t, CSL_E_INVALID, "boot_fit=1 supports at most 768 sphere samples");
         }
@@ -432,7 +442,7 @@ int csl_create(const csl_params *params, const csl_inputs *inputs, int device, c
             P.delta_q = t->delta_q.p;
             P.sampling = t->sampling.p;
             P.b0s_mask = t->b0s.p;
-            if (p.boot_fit == 1) {
+            if (p.boot_fit >= 1) {
                 if (hr > 160)
                     return fail(t, CSL_E_INVALID, "boot_fit=1 supports at most 160 non-b0 volumes, got %d", hr);
                 // volume order of the batched gather: non-b0 volumes, then b0s
@@ -480,6 +490,10 @@ int csl_create(const csl_params *params, const csl_inputs *inputs, int device, c
                 const size_t slots = (size_t)t->nsm * 128;
                 CK(t->bb_odf.ensure(slots * g.vstride));
                 CK(t->bb_pts.ensure(slots * (size_t)p.max_sline_len * 3));
+                CK(t->bb_rng_save.ensure(slots * 4 * 5));
+                CK(t->bb_refit_scr.ensure((size_t)t->nsm * 16 * kRefitScr));
+                CK(t->bb_refit_count.ensure(2));
+                CK(cudaMemsetAsync(t->bb_refit_count.p, 0, 2 * sizeof(unsigned long long), t->own_stream));
             }
         }
         if (p.model == PROB) {
@@ -571,6 +585,17 @@ int csl_destroy(csl_tracker *t) {
 // (the per-warp path recomputes them).
 static constexpr int kUsePerWarpPath = 1;
 
+// Near-tie re-evaluation of the batched fit: on for boot_fit = 1, off for 2.
+// The flag margin is 2e-4 of the row maximum, 7x the largest BF16x3 ODF error
+// measured against float64 (2.9e-5).
+static void set_refit(csl_tracker *t, BootBatchArgs &A) {
+    A.refit = t->hp.boot_fit == 1 ? 1 : 0;
+    A.refit_tol = 2e-4f;
+    A.rng_save = t->bb_rng_save.p;
+    A.refit_scr = t->bb_refit_scr.p;
+    A.refit_count = t->bb_refit_count.p;
+}
+
 static int run_boot_batch(csl_tracker *t, const float *seeds_dev, int ni, int nsl, long long rng_base,
                           cudaStream_t st) {
     const DevParams &P = t->P;
@@ -610,6 +635,7 @@ static int run_boot_batch(csl_tracker *t, const float *seeds_dev, int ni, int ns
         A.half_len = t->bb_half_len.p;
         A.half_off = t->bb_half_off.p;
         A.status = t->status.p;
+        set_refit(t, A);
         CK(cudaMemsetAsync(t->bb_hq.p, 0, sizeof(int), st));
         CK(cudaMemsetAsync(t->status.p, 0, sizeof(int), st));
         CK(cudaMemsetAsync(t->pool_count.p, 0, sizeof(unsigned long long), st));
@@ -701,7 +727,7 @@ static int run_batch(csl_tracker *t, const float *seeds_dev, long long n, long l
     CK(t->out_src.ensure((size_t)nsl + 1));
     CK(t->pt_off.ensure((size_t)nsl + 1));
 
-    if (t->hp.boot_fit == 1 && !per_warp_fit && (P.model == CSA || P.model == OPDT)) {
+    if (t->hp.boot_fit >= 1 && !per_warp_fit && (P.model == CSA || P.model == OPDT)) {
         const int r = run_boot_batch(t, seeds_dev, ni, nsl, rng_base, st);
         if (r != kUsePerWarpPath) return r;
     }
@@ -789,14 +815,14 @@ static int run_batch(csl_tracker *t, const float *seeds_dev, long long n, long l
     return CSL_OK;
 }
 
-int csl_boot_odf(csl_tracker *t, const float *points_dev, const int *resample_dev, long long n, int fit,
-                 float *odf_dev, int odf_stride, void *stream) {
+static int boot_probe(csl_tracker *t, const float *points_dev, const int *resample_dev, long long n, int fit,
+                      float *odf_dev, int odf_stride, const float *dirs_dev, float *step_dev, void *stream) {
     if (!t) return fail(nullptr, CSL_E_INVALID, "NULL tracker");
     const DevParams &P = t->P;
     if (P.model != CSA && P.model != OPDT) return fail(t, CSL_E_STATE, "csl_boot_odf needs a bootstrap tracker");
     if (n < 0 || n > (1ll << 30)) return fail(t, CSL_E_INVALID, "bad point count");
     if (fit != 0 && fit != 1) return fail(t, CSL_E_INVALID, "fit must be 0 or 1");
-    if (fit == 1 && t->hp.boot_fit != 1)
+    if (fit == 1 && t->hp.boot_fit < 1)
         return fail(t, CSL_E_STATE, "fit=1 needs a tracker created with boot_fit=1");
     if (odf_stride < P.samplm_nr || odf_stride % 4 != 0)
         return fail(t, CSL_E_INVALID, "odf_stride must be >= samplm_nr and a multiple of 4");
@@ -825,6 +851,9 @@ int csl_boot_odf(csl_tracker *t, const float *points_dev, const int *resample_de
         A.probe_idx = resample_dev;
         A.probe_odf = odf_dev;
         A.probe_stride = odf_stride;
+        set_refit(t, A);
+        A.probe_dirs = dirs_dev;
+        A.probe_step = step_dev;
         CK(cudaMemsetAsync(t->bb_hq.p, 0, sizeof(int), st));
         CK(cudaMemsetAsync(t->status.p, 0, sizeof(int), st));
         CK(launch_boot_batch(P, g, A, t->partner.p, t->nsm, st));
@@ -833,6 +862,31 @@ int csl_boot_odf(csl_tracker *t, const float *points_dev, const int *resample_de
     CK(cudaStreamSynchronize(st));
     if (fit == 1 && ((int)(t->host_stage[0] & 0xffffffff) & ST_WAIT_TIMEOUT))
         return fail(t, CSL_E_KERNEL, "tensor-core pipeline wait timed out");
+    return CSL_OK;
+}
+
+int csl_boot_odf(csl_tracker *t, const float *points_dev, const int *resample_dev, long long n, int fit,
+                 float *odf_dev, int odf_stride, void *stream) {
+    return boot_probe(t, points_dev, resample_dev, n, fit, odf_dev, odf_stride, nullptr, nullptr, stream);
+}
+
+int csl_boot_step(csl_tracker *t, const float *points_dev, const int *resample_dev, const float *dirs_dev,
+                  long long n, float *odf_dev, int odf_stride, float *step_dev, void *stream) {
+    if (!t) return fail(nullptr, CSL_E_INVALID, "NULL tracker");
+    if (t->hp.boot_fit < 1) return fail(t, CSL_E_STATE, "csl_boot_step needs a tracker created with boot_fit >= 1");
+    if (n > 0 && (!dirs_dev || !step_dev)) return fail(t, CSL_E_INVALID, "NULL buffer");
+    return boot_probe(t, points_dev, resample_dev, n, 1, odf_dev, odf_stride, dirs_dev, step_dev, stream);
+}
+
+int csl_boot_refit_stats(csl_tracker *t, unsigned long long *out2, int reset) {
+    if (!t) return fail(nullptr, CSL_E_INVALID, "NULL tracker");
+    if (t->hp.boot_fit < 1) return fail(t, CSL_E_STATE, "no batched fit on this tracker");
+    CK(cudaSetDevice(t->device));
+    if (out2)
+        CK(cudaMemcpyAsync(out2, t->bb_refit_count.p, 2 * sizeof(unsigned long long), cudaMemcpyDeviceToHost,
+                           t->own_stream));
+    if (reset) CK(cudaMemsetAsync(t->bb_refit_count.p, 0, 2 * sizeof(unsigned long long), t->own_stream));
+    CK(cudaStreamSynchronize(t->own_stream));
     return CSL_OK;
 }
 

@@ -94,7 +94,19 @@ struct BootBatchArgs {
     int *half_len;             // [2 nsl] points per half (seed included)
     long long *half_off;       // [2 nsl] pool offset of each half (-1 when the pool overflowed)
     int *status;
+    // near-tie re-evaluation (refit != 0): a row whose peak decisions lie within
+    // refit_tol x (row maximum) of flipping is fitted again in float64 and searched
+    // again before the closest peak is chosen
+    int refit;
+    float refit_tol;
+    uint32_t *rng_save;                 // [grid * 128 * 4][5]: Philox counter and index at each attempt's draws
+    double *refit_scr;                  // [grid * 16 warps][kRefitScr] float64 scratch
+    unsigned long long *refit_count;    // [2]: rows searched, rows fitted again
+    // probe mode with directions: the chosen step of each probe item
+    const float *probe_dirs;            // [nprobe, 3] incoming directions (NULL: ODF rows only)
+    float *probe_step;                  // [nprobe, 4]: direction, found + 2 * (row fitted again)
 };
+constexpr int kRefitScr = 2048;         // doubles of float64 scratch per warp
 
 BootBatchGeom boot_batch_geom(const DevParams &P, int hr, int nb0);
 cudaError_t launch_boot_batch_pack(const DevParams &P, const BootBatchGeom &g, void *B1g, void *B2g,

@@ -10,6 +10,7 @@ contributes its fields of the C ABI's ``csl_params`` / ``csl_inputs``.
 
 from __future__ import annotations
 
+import ctypes as C
 import logging
 import math
 from abc import ABC
@@ -60,10 +61,12 @@ class BootDirectionGetter(GPUDirectionGetter):
                  b0s_mask: np.ndarray, *, fit: str = "fp32"):
         """``fit`` (keyword only, not in the reference): "fp32" runs the
         reference's per-warp FP32 fit with identical results; "bf16x3" runs the
-        batched tensor-core fit (CSA model), 128 streamline halves per CTA with
-        BF16x3 products and FP32 accumulation."""
-        if fit not in ("fp32", "bf16x3"):
-            raise ValueError(f"Invalid fit {fit!r}, must be one of 'fp32', 'bf16x3'")
+        batched tensor-core fit (CSA or OPDT), 128 streamline halves per CTA with
+        BF16x3 products and FP32 accumulation, and fits again in float64 any row
+        whose peak decisions lie within the BF16x3 error of flipping;
+        "bf16x3_nofp64" is the batched fit without that re-evaluation."""
+        if fit not in ("fp32", "bf16x3", "bf16x3_nofp64"):
+            raise ValueError(f"Invalid fit {fit!r}, must be one of 'fp32', 'bf16x3', 'bf16x3_nofp64'")
         self.fit = fit
         if model_type.upper() == "OPDT":
             self.model_type = _lib.MODEL_OPDT
@@ -104,7 +107,7 @@ class BootDirectionGetter(GPUDirectionGetter):
         if len(self.b0s_mask) != tracker.dimt:
             raise ValueError("b0s_mask length must match the last dimension of dataf")
         params.model = self.model_type
-        params.boot_fit = 1 if self.fit == "bf16x3" else 0
+        params.boot_fit = {"fp32": 0, "bf16x3": 1, "bf16x3_nofp64": 2}[self.fit]
         params.min_signal = float(self.min_signal)
         params.delta_nr = self.delta_nr
         params.samplm_nr = int(self.sampling_matrix.shape[0])
@@ -151,13 +154,53 @@ class PttDirectionGetter(ProbDirectionGetter):
         self.target_short_step = target_short_step
 
     def prepare_data(self, dataf, stop_map, stop_threshold, sphere_vertices, sphere_symm):
-        """Normalise and tile the ODF for the texture, and build the vertex LUT.
+        """Normalise and tile the ODF for the texture, and build the vertex LUT,
+        on the GPU (``csl_ptt_prepare``; device ``self.device``, default 0).
 
         Same transformation as ``cu_direction_getters.py:531-625``: clip at 0,
         zero outside the tracking mask, normalise each voxel to max 1, tile
         the vertex axis over (nx, ny, nz) power-of-two tiles, and map a
-        ``res^3`` grid on [-1, 1]^3 to the nearest sphere vertex.
+        ``res^3`` grid on [-1, 1]^3 to the nearest sphere vertex.  Returns the
+        tiled data as a ``DeviceBuffer`` (``.numpy()`` copies it to the host);
+        equal to ``prepare_data_host`` bit for bit except at exact vertex
+        distance ties of the LUT.
         """
+        dataf = np.ascontiguousarray(dataf, dtype=np.float32)
+        X, Y, Z, T = dataf.shape
+        lib = _lib.load()
+        lay = [C.c_int() for _ in range(5)]
+        _lib.check(lib.csl_ptt_layout(T, *[C.byref(x) for x in lay]))
+        self.nx, self.ny, self.nz, self.log2_x, self.log2_y = (x.value for x in lay)
+        dev = int(getattr(self, "device", 0))
+        verts = np.ascontiguousarray(sphere_vertices, dtype=np.float32)
+        # the host computation compares stop_map < stop_threshold with numpy's
+        # promotion: in float32 for a Python or float32 threshold
+        thr = np.asarray(stop_threshold)
+        thr = float(np.float32(thr)) if np.result_type(np.float32, stop_threshold) == np.float32 else float(thr)
+        odf = _lib.DeviceBuffer.from_array(dataf, dev)
+        stop = _lib.DeviceBuffer.from_array(np.ascontiguousarray(stop_map, dtype=np.float32), dev)
+        vd = _lib.DeviceBuffer.from_array(verts, dev)
+        tiled = _lib.DeviceBuffer(dev, (self.nz * Z, self.ny * Y, self.nx * X), np.float32)
+        res = int(self.odf_lut_res)
+        lut = _lib.DeviceBuffer(dev, (res, res, res), np.float32)
+        rc = lib.csl_ptt_prepare(C.c_void_p(odf.ptr), C.c_void_p(stop.ptr), X, Y, Z, T, thr, C.c_void_p(vd.ptr),
+                                 len(verts), 1 if sphere_symm else 0, res, C.c_void_p(tiled.ptr),
+                                 C.c_void_p(lut.ptr), None)
+        _lib.check(rc)
+        _lib.device_sync(dev)
+        for b in (odf, stop, vd):
+            b.close()
+        logger.info("PTT ODF texture %dx%dx%d (%.2f GB), prepared on GPU %d", self.nx * X, self.ny * Y,
+                    self.nz * Z, tiled.nbytes / 1e9, dev)
+        self._lut_dev = lut
+        self.sphere_vertices_lut_h = None
+        return tiled
+
+    def prepare_data_host(self, dataf, stop_map, stop_threshold, sphere_vertices, sphere_symm):
+        """The host computation of ``prepare_data`` (numpy + a KD-tree), as the
+        reference runs it (``cu_direction_getters.py:531-625``); returns the
+        tiled array and sets ``sphere_vertices_lut_h``.  The library's own path
+        is ``prepare_data`` (on the GPU); this one serves the CPU oracle."""
         from scipy.spatial import cKDTree
 
         dimx, dimy, dimz, dimt = dataf.shape
@@ -201,7 +244,10 @@ class PttDirectionGetter(ProbDirectionGetter):
         return tiled
 
     def fill(self, params, inputs, tracker, keep):
-        if self.sphere_vertices_lut_h is None:
+        lut = getattr(self, "_lut_dev", None)
+        if lut is None:
+            lut = self.sphere_vertices_lut_h
+        if lut is None:
             raise RuntimeError("PttDirectionGetter.prepare_data must run before allocation")
         params.model = _lib.MODEL_PTT
         params.samplm_nr = tracker.dimt
@@ -213,6 +259,6 @@ class PttDirectionGetter(ProbDirectionGetter):
         params.tile_log2_x, params.tile_log2_y = self.log2_x, self.log2_y
         params.tile_nx, params.tile_ny, params.tile_nz = self.nx, self.ny, self.nz
         keep.append(tracker.dataf)
-        keep.append(self.sphere_vertices_lut_h)
-        inputs.ptt_odf_tiled = _lib.fptr(tracker.dataf)
-        inputs.ptt_lut = _lib.fptr(self.sphere_vertices_lut_h)
+        keep.append(lut)
+        inputs.ptt_odf_tiled = _lib.any_fptr(tracker.dataf)
+        inputs.ptt_lut = _lib.any_fptr(lut)

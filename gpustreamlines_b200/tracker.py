@@ -50,6 +50,7 @@ class GPUTracker(GenericTracker):
         """
         self.dimx, self.dimy, self.dimz, self.dimt = (int(d) for d in np.shape(dataf))
         if hasattr(dg, "prepare_data"):
+            dg.device = int(device_offset)  # the getter's data preparation runs on the first GPU
             self.dataf = dg.prepare_data(np.array(dataf, dtype=np.float32), stop_map, stop_threshold,
                                          sphere_vertices, sphere_symm)
         else:

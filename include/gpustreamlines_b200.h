@@ -69,8 +69,11 @@ typedef struct csl_params {
     int boot_fit;                 /* bootstrap fit: 0 = one warp per streamline in FP32 with the
                                      reference's arithmetic (results identical to it); 1 = batched
                                      fit on the tensor cores in BF16x3 with FP32 accumulation, 128
-                                     streamline halves per CTA (CSA or OPDT; no counterpart in the
-                                     reference, whose getter is the per-warp one, boot.cu:393-608) */
+                                     streamline halves per CTA, rows whose peak decisions lie within
+                                     2e-4 of the row maximum of flipping fitted again in float64
+                                     (CSA or OPDT; no counterpart in the reference, whose getter is
+                                     the per-warp one, boot.cu:393-608); 2 = as 1 without the
+                                     float64 re-evaluation */
     /* PTT getter (PttDirectionGetter, cu_direction_getters.py:417-468) */
     int odf_lut_res;              /* nearest-vertex LUT resolution (128) */
     int step_frac;                /* STEP_FRAC = round(step / target_short_step) */
@@ -106,8 +109,10 @@ typedef struct csl_inputs {
     const float *sampling_matrix; /* [samplm_nr,delta_nr] */
     const int *b0s_mask;          /* [T] 1 where the volume is a b0 */
     /* PTT only (NULL otherwise) */
-    const float *ptt_odf_tiled;   /* [nz*Z, ny*Y, nx*X] tiled, normalised ODF texture data */
-    const float *ptt_lut;         /* [res,res,res] nearest-vertex index, stored as float */
+    const float *ptt_odf_tiled;   /* [nz*Z, ny*Y, nx*X] tiled, normalised ODF texture data (host or
+                                     device memory, e.g. from csl_ptt_prepare) */
+    const float *ptt_lut;         /* [res,res,res] nearest-vertex index, stored as float (host or
+                                     device memory) */
 } csl_inputs;
 
 /* Create a tracker on `device`: validate, upload inputs, build textures and
@@ -241,6 +246,20 @@ int csl_boot_odf(csl_tracker *tracker, const float *points_dev, const int *resam
                  float *odf_dev, int odf_stride, void *stream);
 
 /*
+ * The batched fit's step at fixed state (measurement entry point, no
+ * counterpart in the reference): as csl_boot_odf with fit = 1, plus the peak
+ * search and closest-peak choice for the incoming direction dirs_dev[i]
+ * (float32 [n,3]), the near-tie float64 re-evaluation included when the
+ * tracker has boot_fit = 1.  step_dev[i] (float32 [n,4]) = the new direction,
+ * and in .w: 1 if a peak was found, + 2 if the row was fitted again in float64.
+ * csl_boot_refit_stats reads {rows searched, rows fitted again} of the batched
+ * fit since creation or the last reset (reset != 0 zeroes them).
+ */
+int csl_boot_step(csl_tracker *tracker, const float *points_dev, const int *resample_dev, const float *dirs_dev,
+                  long long n, float *odf_dev, int odf_stride, float *step_dev, void *stream);
+int csl_boot_refit_stats(csl_tracker *tracker, unsigned long long *out2, int reset);
+
+/*
  * ODF / PMF volume from SH coefficients on the tensor cores (the host step
  * before tracking in run_gpu_streamlines.py:357-380, fit.odf(sphere) clipped
  * to >= 0 for the probabilistic getter):
@@ -369,6 +388,28 @@ int csl_set_launch(csl_tracker *t, int threads_per_block, int seed_order);
 int csl_get_launch(csl_tracker *t, int *threads_per_block, int *seed_order, int *blocks_per_sm);
 int csl_autotune(csl_tracker *t, const float *seeds_dev, long long n, long long rng_index_base, int repeats,
                  float *ms_out);
+
+/*
+ * PTT data preparation on the device (replaces the host step of
+ * PttDirectionGetter.prepare_data, cu_direction_getters.py:531-625).
+ *   csl_ptt_layout   power-of-two tiles (nx, ny, nz) of the texture's vertex
+ *                    axis for T vertices, and log2 of nx, ny
+ *   csl_ptt_prepare  DEVICE buffers: odf [X,Y,Z,T], stop map [X,Y,Z], sphere
+ *                    vertices [V,3] in; out the tiled, normalised texture data
+ *                    [nz*Z][ny*Y][nx*X] (ODF clipped at 0, zeroed where
+ *                    stop < stop_threshold, each voxel divided by its
+ *                    maximum) and the nearest-vertex LUT [res][res][res]
+ *                    (index as float; grid numpy.linspace(-1, 1, res) per
+ *                    axis; with sphere_symm the nearer of +-v).  Both equal
+ *                    the host computation bit for bit except that exact
+ *                    distance ties take the lower vertex index.  Enqueued on
+ *                    `stream`.  csl_create accepts these device buffers as
+ *                    csl_inputs.ptt_odf_tiled / ptt_lut directly.
+ */
+int csl_ptt_layout(int T, int *nx, int *ny, int *nz, int *log2_x, int *log2_y);
+int csl_ptt_prepare(const float *odf_dev, const float *stop_dev, int X, int Y, int Z, int T, double stop_threshold,
+                    const float *verts_dev, int V, int sphere_symm, int lut_res, float *tiled_dev, float *lut_dev,
+                    void *stream);
 
 /*
  * Device plumbing for hosts without a CUDA runtime binding of their own (the

@@ -45,7 +45,7 @@ def main():
                    vertices=np.ascontiguousarray(sph.vertices, dtype=np.float32),
                    edges=np.ascontiguousarray(sph.edges, dtype=np.int32))
         dg = PttDirectionGetter()
-        tiled = dg.prepare_data(pmf, inp["stop_map"], np.float32(0.1), inp["vertices"], False)
+        tiled = dg.prepare_data_host(pmf, inp["stop_map"], np.float32(0.1), inp["vertices"], False)
         ptt = dict(tiled=tiled, lut=dg.sphere_vertices_lut_h, res=dg.odf_lut_res)
     else:
         inp = cases.inputs(name)

@@ -156,7 +156,7 @@ def ptt_layout(name):
     c = CASES[name]
     inp = inputs(name)
     dg = PttDirectionGetter()
-    tiled = dg.prepare_data(inp["dataf"].copy(), inp["stop_map"], np.float32(c["fa_thr"]),
+    tiled = dg.prepare_data_host(inp["dataf"].copy(), inp["stop_map"], np.float32(c["fa_thr"]),
                             inp["vertices"], False)
     return dict(tiled=tiled, lut=dg.sphere_vertices_lut_h, log2_x=dg.log2_x, log2_y=dg.log2_y,
                 nx=dg.nx, ny=dg.ny, nz=dg.nz, res=dg.odf_lut_res)
