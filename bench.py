@@ -48,9 +48,10 @@ BYTES_PER_STEP = 8 * 724 * 4 + 8 * 4 + 12  # PMF corners + stop-map taps + point
 # capture of this workload at 20,000 seeds (27.25 GB over 6,372,721 steps, see
 # profiles/track_kernel_prob_81x106x76x724.md); scaled to a full launch by steps.
 TRAFFIC_BYTES_PER_STEP = 4277.0
-# The same for track_kernel<PROB_ENV> (envelope sampler): 6.90 GB over 6,341,719
-# steps at 20,000 seeds (profiles/track_kernel_prob_env_81x106x76x724.md).
-ENV_TRAFFIC_BYTES_PER_STEP = 1088.0
+# The same for track_kernel<PROB_ENV> (envelope sampler, four draws per round):
+# 9.83 GB over 6,349,590 steps at 20,000 seeds
+# (profiles/track_kernel_prob_env_81x106x76x724.md).
+ENV_TRAFFIC_BYTES_PER_STEP = 1547.4
 
 
 def parse():
@@ -189,22 +190,26 @@ def plain_arm(args, data, ph, sph, gcfg, seeds_d, local, stream, barrier, dist, 
 
 
 def run_boot_compare(args):
-    """Bootstrap CSA (sh_order 8, 45 coefficients, 81x106x76x160 DWI) at --seeds:
-    the batched BF16x3 tensor-core fit and the per-warp FP32 fit (the reference's
-    arithmetic), each timed device-resident (pass 1 + pass 2 + compaction) after
-    a 10,000-seed warm-up batch, with the tensor roofline of the batched fit."""
-    from gpustreamlines_b200 import _lib, Tracker
+    """Bootstrap CSA (sh_order 8, 45 coefficients, 81x106x76x160 DWI) at --seeds,
+    three pass-2 forms in one run: the batched BF16x3 tensor-core fit with the
+    float64 re-fit of near-tie rows (boot_fit 1, the default batched form), the
+    same without the re-fit (boot_fit 2), and the per-warp FP32 fit (the
+    reference's arithmetic).  Each is timed device-resident (pass 1 + pass 2 +
+    compaction) after one untimed batch of the same seeds (which sizes the point
+    pool), with the tensor roofline of the batched fit and its re-fit counts."""
+    from gpustreamlines_b200 import _lib, Tracker, BootDirectionGetter
 
     ph, sph, data, seeds = build_workload(0, args.seeds, "csa_bf16x3")
     d = _lib.DeviceBuffer.from_array(seeds, 0)
-    warm = _lib.DeviceBuffer.from_array(seeds[:10000], 0)
     out = {}
-    for fit in ("bf16x3", "fp32"):
-        dg = make_getter("csa_bf16x3" if fit == "bf16x3" else "csa", ph, sph)
+    for fit in ("bf16x3", "bf16x3_nofp64", "fp32"):
+        dg = BootDirectionGetter.from_dipy_csa(ph.gtab, sph, sh_order_max=8, fit=fit)
         with Tracker(dg, data, ph.fa, 0.1, sph.vertices, sph.edges, max_angle=math.radians(60), step_size=0.5) as tr:
             h = tr.handles[0]
-            h.propagate_device(warm.ptr, 10000, 0, None)
-            reps = args.steps if fit == "bf16x3" else 1
+            h.propagate_device(d.ptr, len(seeds), 0, None)
+            if fit != "fp32":
+                h.boot_refit_stats(reset=True)
+            reps = args.steps if fit != "fp32" else 1
             with ClockSampler(0) as clk:
                 t0 = time.perf_counter()
                 ms = []
@@ -219,7 +224,10 @@ def run_boot_compare(args):
             out[fit] = {"steps": int(npts - nsl), "streamlines": int(nsl), "batch_ms": tot, "pass2_ms": p2,
                         "steps_per_s": (npts - nsl) / (tot / 1e3), "batches": reps, "wall_s": wall,
                         "clocks": clk.summary()}
-            if fit == "bf16x3":
+            if fit != "fp32":
+                st = h.boot_refit_stats()
+                out[fit]["rows_searched"] = st["rows"]
+                out[fit]["rows_fitted_again_fp64"] = st["refit"]
                 nc = dg.delta_nr
                 hr = int((dg.b0s_mask == 0).sum())
                 flop = 2 * 2 * hr * hr + 2 * nc * hr + 2 * nc * dg.sampling_matrix.shape[0]
@@ -231,7 +239,8 @@ def run_boot_compare(args):
                                         "issued_bf16_flop_per_step": 3 * flop,
                                         "peak_source": "measured MEASURED_PEAKS bf16_tflops"}
     print(json.dumps({"workload": f"bootstrap CSA getter, sh_order 8 (45 coeffs), 81x106x76x160 DWI, {args.seeds} seeds, "
-                                  "step 0.5, max angle 60", "batched_bf16x3": out["bf16x3"], "per_warp_fp32": out["fp32"],
+                                  "step 0.5, max angle 60", "batched_bf16x3": out["bf16x3"],
+                      "batched_bf16x3_without_fp64_refit": out["bf16x3_nofp64"], "per_warp_fp32": out["fp32"],
                       "speedup_bf16x3_vs_fp32": out["bf16x3"]["steps_per_s"] / out["fp32"]["steps_per_s"]}),
           flush=True)
     return 0

@@ -141,34 +141,53 @@ __global__ void boot_batch_dwi_kernel(const float *__restrict__ src, const int *
     }
 }
 
-// streamline -> (seed, initial vertex) from the pass-1 outputs
+// streamline -> (seed, initial vertex) from the pass-1 outputs; streamlines
+// at or past cap (the slot capacity of a graph-captured batch) are not
+// written and flag ST_SLOT_OVERFLOW
 __global__ void boot_batch_prep_kernel(const int *__restrict__ npeaks, const int *__restrict__ sl_off,
-                                       const short *__restrict__ peaks, int max_store, int n,
+                                       const short *__restrict__ peaks, int max_store, int n, int cap,
                                        int *sl_seed, short *sl_vert, int *status) {
     for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < n; s += gridDim.x * blockDim.x) {
         const int np = npeaks[s], base = sl_off[s];
         if (np > max_store) atomicOr(status, ST_PEAKS_OVERFLOW);
         const int m = np < max_store ? np : max_store;
         for (int k = 0; k < m; k++) {
+            if (base + k >= cap) {
+                atomicOr(status, ST_SLOT_OVERFLOW);
+                break;
+            }
             sl_seed[base + k] = s;
             sl_vert[base + k] = peaks[(size_t)s * max_store + k];
         }
     }
 }
 
+// the streamline count of a batch: nsl, or min(*count, nsl) when the count is
+// in device memory (graph-captured batches, nsl = their slot capacity)
+__device__ __forceinline__ int batch_count(const int *count, int nsl) {
+    if (!count) return nsl;
+    const int c = *count;
+    return c < 0 ? 0 : (c < nsl ? c : nsl);
+}
+
 // streamline length = backward half + forward half - the shared seed point
 __global__ void boot_batch_join_kernel(const int *__restrict__ half_len, const int *__restrict__ sl_seed,
-                                       int nsl, int *out_len, int *out_seed) {
+                                       int nsl, const int *__restrict__ count, int *out_len, int *out_seed) {
+    nsl = batch_count(count, nsl);
     for (int sl = blockIdx.x * blockDim.x + threadIdx.x; sl < nsl; sl += gridDim.x * blockDim.x) {
         out_len[sl] = half_len[2 * sl] - 1 + half_len[2 * sl + 1];
         out_seed[sl] = sl_seed[sl];
     }
 }
 
-// reversed backward half, then the forward half without its seed point
+// reversed backward half, then the forward half without its seed point;
+// nothing when the batch's status shows an overflow (it is re-run)
 __global__ void gather_halves_kernel(const float *__restrict__ pool, const long long *__restrict__ half_off,
                                      const int *__restrict__ half_len, const long long *__restrict__ pt_off,
-                                     int nsl, float *__restrict__ out) {
+                                     int nsl, const int *__restrict__ count, const int *__restrict__ status,
+                                     float *__restrict__ out) {
+    if (status && (*status & (ST_POOL_OVERFLOW | ST_SLOT_OVERFLOW | ST_PEAKS_OVERFLOW))) return;
+    nsl = batch_count(count, nsl);
     const int lane = threadIdx.x & 31;
     const int wpb = blockDim.x / kWarp;
     for (int sl = blockIdx.x * wpb + threadIdx.x / kWarp; sl < nsl; sl += gridDim.x * wpb) {
@@ -494,16 +513,33 @@ __device__ __forceinline__ bool near_tie(const DevParams &P, const float *odf, c
 // h + r[idx], clamp at min_signal, division by the mean clamped b0 signal, the
 // CSA transform (coefficient 0 fixed) or the OPDT form, and the sphere
 // sampling; the row is rounded to float into odf.  Arithmetic of the float64
-// accuracy reference (oracle/fp64.py).  scr: kRefitScr doubles of this warp.
+// accuracy reference (oracle/fp64.py).
+//
+// Layout for speed: vectors over the hr non-b0 volumes live in registers,
+// element j in lane j % 32, slot j / 32 (hr <= 160), and are broadcast with
+// shuffles; the matrices come from the float64 tables of refit_tab_layout,
+// transposed so that a warp's 32 lanes read 32 consecutive entries.  idx:
+// hr ints of this warp's scratch.
+constexpr int kRefitJ = 5;  // register slots per lane for an hr-vector (hr <= 160)
+
+__device__ __forceinline__ double shfl_d(double x, int src) { return __shfl_sync(FULL, x, src); }
+
+// element i of a register-distributed hr-vector (i warp-uniform)
+__device__ __forceinline__ double bcast(const double (&x)[kRefitJ], int i) {
+    double r = 0.0;
+#pragma unroll
+    for (int k = 0; k < kRefitJ; k++)
+        if ((i >> 5) == k) r = x[k];
+    return shfl_d(r, i & 31);
+}
+
 __device__ __noinline__ void boot_refit_fp64(const DevParams &P, int hr, int nblk1, const int *__restrict__ volidx,
-                                             float4 pt4, const int *pidx, const uint32_t *saved, double *scr,
-                                             float *odf, int lane) {
+                                             float4 pt4, const int *pidx, const uint32_t *saved,
+                                             const double *__restrict__ tab, int *idx, float *odf, int lane) {
     const int T = P.dimt, C = P.delta_nr, V = P.samplm_nr;
-    double *full = scr;                                        // [T]
-    double *rr = scr + 512;                                    // [hr] residuals, then the transform
-    double *hh = scr + 1024;                                   // [hr] fitted, then the bootstrap signal
-    double *cf = scr + 1536;                                   // [C]
-    int *idx = reinterpret_cast<int *>(scr + 1600);            // [hr]
+    const RefitTab L = refit_tab_layout(hr, C, V);
+    const double2 *rh = reinterpret_cast<const double2 *>(tab + L.rh);
+    const double *dq = tab + L.dq, *db = tab + L.db, *smp = tab + L.smp;
     const double px = pt4.x, py = pt4.y, pz = pt4.z;
     const bool inb = (px >= -0.5) && (px + 0.5 < P.dimx) && (py >= -0.5) && (py + 0.5 < P.dimy) &&
                      (pz >= -0.5) && (pz + 0.5 < P.dimz);
@@ -511,34 +547,6 @@ __device__ __noinline__ void boot_refit_fp64(const DevParams &P, int hr, int nbl
         for (int v = lane; v < V; v += kWarp) odf[v] = 0.0f;
         __syncwarp();
         return;
-    }
-    // trilinear interpolation in double (corners in (i, j, k) order)
-    const double fx = floor(px), fy = floor(py), fz = floor(pz);
-    const double wx = px - fx, wy = py - fy, wz = pz - fz;
-    const int lx = fx < 0 ? 0 : (int)fx, ly = fy < 0 ? 0 : (int)fy, lz = fz < 0 ? 0 : (int)fz;
-    const int hx = min(lx + 1, P.dimx - 1), hy = min(ly + 1, P.dimy - 1), hz = min(lz + 1, P.dimz - 1);
-    for (int t = lane; t < T; t += kWarp) {
-        double acc = 0.0;
-#pragma unroll
-        for (int q = 0; q < 8; q++) {
-            const int i = q >> 2, j = (q >> 1) & 1, k = q & 1;
-            const double w = __dmul_rn(__dmul_rn(i ? wx : 1.0 - wx, j ? wy : 1.0 - wy), k ? wz : 1.0 - wz);
-            const long long vx = ((long long)(i ? hx : lx) * P.dimy + (j ? hy : ly)) * P.dimz + (k ? hz : lz);
-            acc = __dadd_rn(acc, __dmul_rn(w, (double)__ldg(P.dataf + vx * T + t)));
-        }
-        full[t] = acc;
-    }
-    __syncwarp();
-    // residual and hat products over the non-b0 volumes (volidx[0..hr))
-    for (int j = lane; j < hr; j += kWarp) {
-        double r = 0.0, h = 0.0;
-        for (int i = 0; i < hr; i++) {
-            const double s = full[volidx[i]];
-            r = fma((double)__ldg(P.R + (size_t)j * hr + i), s, r);
-            h = fma((double)__ldg(P.H + (size_t)j * hr + i), s, h);
-        }
-        rr[j] = r;
-        hh[j] = h;
     }
     // resample indices: given, or the batched fit's draws (part p drew columns
     // 16b .. 16b+15 for b = p, p + 4, ... in order)
@@ -554,59 +562,128 @@ __device__ __noinline__ void boot_refit_fp64(const DevParams &P, int hr, int nbl
             for (int e = 0; e < 16; e++)
                 if (16 * b + e < hr) idx[16 * b + e] = (int)(g.next() % (unsigned)hr);
     }
-    __syncwarp();
-    for (int j = lane; j < hr; j += kWarp) hh[j] = hh[j] + rr[idx[j]];
-    __syncwarp();
-    for (int j = lane; j < hr; j += kWarp) full[volidx[j]] = hh[j];
-    __syncwarp();
-    // clamp, b0 mean of the clamped signal, normalise
+    // trilinear interpolation in double (corners in (i, j, k) order) of volume t
+    const double fx = floor(px), fy = floor(py), fz = floor(pz);
+    const double wx = px - fx, wy = py - fy, wz = pz - fz;
+    const int lx = fx < 0 ? 0 : (int)fx, ly = fy < 0 ? 0 : (int)fy, lz = fz < 0 ? 0 : (int)fz;
+    const int hx = min(lx + 1, P.dimx - 1), hy = min(ly + 1, P.dimy - 1), hz = min(lz + 1, P.dimz - 1);
+    auto interp = [&](int t) {
+        double acc = 0.0;
+#pragma unroll
+        for (int q = 0; q < 8; q++) {
+            const int i = q >> 2, j = (q >> 1) & 1, k = q & 1;
+            const double w = __dmul_rn(__dmul_rn(i ? wx : 1.0 - wx, j ? wy : 1.0 - wy), k ? wz : 1.0 - wz);
+            const long long vx = ((long long)(i ? hx : lx) * P.dimy + (j ? hy : ly)) * P.dimz + (k ? hz : lz);
+            acc = __dadd_rn(acc, __dmul_rn(w, (double)__ldg(P.dataf + vx * T + t)));
+        }
+        return acc;
+    };
     const double ms = (double)P.min_signal;
+    double sv[kRefitJ];
+#pragma unroll
+    for (int k = 0; k < kRefitJ; k++) {
+        const int j = lane + 32 * k;
+        sv[k] = j < hr ? interp(__ldg(volidx + j)) : 0.0;
+    }
+    // b0 mean of the clamped signal (the b0 volumes are not resampled)
     double bs = 0.0;
-    int nb = 0;
-    for (int t = lane; t < T; t += kWarp) {
-        const double x = full[t] > ms ? full[t] : ms;
-        full[t] = x;
-        if (__ldg(P.b0s_mask + t)) {
-            bs += x;
-            nb++;
+    for (int j = hr + lane; j < T; j += kWarp) {
+        const double x = interp(__ldg(volidx + j));
+        bs += x > ms ? x : ms;
+    }
+#pragma unroll
+    for (int o = 16; o; o >>= 1) bs += shfl_d(bs, lane ^ o);
+    const double denom = bs / (T - hr);
+    // r = R s and h = H s: lane j accumulates rows j + 32k over i in order
+    double rr[kRefitJ], hh[kRefitJ];
+#pragma unroll
+    for (int k = 0; k < kRefitJ; k++) rr[k] = hh[k] = 0.0;
+    for (int i0 = 0; i0 < hr; i0 += 32) {
+#pragma unroll 4
+        for (int ii = 0; ii < 32; ii++) {
+            const int i = i0 + ii;
+            if (i >= hr) break;
+            double si = 0.0;
+#pragma unroll
+            for (int k = 0; k < kRefitJ; k++)
+                if ((i0 >> 5) == k) si = sv[k];
+            si = shfl_d(si, ii);
+#pragma unroll
+            for (int k = 0; k < kRefitJ; k++) {
+                const int j = lane + 32 * k;
+                if (j < hr) {
+                    const double2 m = __ldg(rh + (size_t)i * hr + j);
+                    rr[k] = fma(m.x, si, rr[k]);
+                    hh[k] = fma(m.y, si, hh[k]);
+                }
+            }
+        }
+    }
+    __syncwarp();  // idx written
+    // bootstrap, clamp, normalise, transform: y = x / denom; CSA: log(-log c),
+    // OPDT: -log y (1.5 + log y) y (y kept for the second product)
+    const bool opdt = P.model == OPDT;
+    double yv[kRefitJ], tv[kRefitJ];
+#pragma unroll
+    for (int k = 0; k < kRefitJ; k++) {
+        const int j = lane + 32 * k;
+        const int src = j < hr ? idx[j] : 0;
+        double rs = 0.0;
+#pragma unroll
+        for (int q = 0; q < kRefitJ; q++) {
+            const double v = shfl_d(rr[q], src & 31);
+            if ((src >> 5) == q) rs = v;
+        }
+        double x = hh[k] + rs;
+        x = x > ms ? x : ms;
+        const double y = x / denom;
+        yv[k] = y;
+        if (opdt) {
+            tv[k] = -log(y) * (1.5 + log(y)) * y;
+        } else {
+            const double c = y < 0.001 ? 0.001 : (y > 0.999 ? 0.999 : y);
+            tv[k] = log(-log(c));
+        }
+        if (j >= hr) yv[k] = tv[k] = 0.0;
+    }
+    // SH coefficients: lane c accumulates c and c + 32 over j in order
+    double cf[2] = {0.0, 0.0}, cb[2] = {0.0, 0.0};
+    for (int j = 0; j < hr; j++) {
+        const double tj = bcast(tv, j);
+        const double yj = opdt ? bcast(yv, j) : 0.0;
+#pragma unroll
+        for (int k = 0; k < 2; k++) {
+            const int c = lane + 32 * k;
+            if (c < C) {
+                cf[k] = fma(__ldg(dq + (size_t)j * kRefitCP + c), tj, cf[k]);
+                if (opdt) cb[k] = fma(__ldg(db + (size_t)j * kRefitCP + c), yj, cb[k]);
+            }
         }
     }
 #pragma unroll
-    for (int o = 16; o; o >>= 1) {
-        bs += __shfl_xor_sync(FULL, bs, o);
-        nb += __shfl_xor_sync(FULL, nb, o);
+    for (int k = 0; k < 2; k++) {
+        const int c = lane + 32 * k;
+        if (opdt) cf[k] -= cb[k];
+        else if (c == 0) cf[k] = 0.28209479177387814;  // 1 / (2 sqrt(pi))
     }
-    const double denom = bs / nb;
-    __syncwarp();
-    const bool opdt = P.model == OPDT;
-    for (int j = lane; j < hr; j += kWarp) {
-        const double y = full[volidx[j]] / denom;
-        hh[j] = y;
-        if (opdt) {
-            rr[j] = -log(y) * (1.5 + log(y)) * y;
-        } else {
-            const double c = y < 0.001 ? 0.001 : (y > 0.999 ? 0.999 : y);
-            rr[j] = log(-log(c));
+    // sphere sampling: lane v accumulates vertices v + 32q over c in order, 8 at a time
+    for (int v0 = 0; v0 < V; v0 += 8 * kWarp) {
+        double o[8];
+#pragma unroll
+        for (int q = 0; q < 8; q++) o[q] = 0.0;
+        for (int c = 0; c < C; c++) {
+            const double cc = shfl_d(c < 32 ? cf[0] : cf[1], c & 31);
+#pragma unroll
+            for (int q = 0; q < 8; q++) {
+                const int v = v0 + lane + 32 * q;
+                if (v < V) o[q] = fma(__ldg(smp + (size_t)c * L.vp + v), cc, o[q]);
+            }
         }
-    }
-    __syncwarp();
-    for (int c = lane; c < C; c += kWarp) {
-        double a = 0.0;
-        for (int j = 0; j < hr; j++) a = fma((double)__ldg(P.delta_q + (size_t)c * hr + j), rr[j], a);
-        if (opdt) {
-            double b = 0.0;
-            for (int j = 0; j < hr; j++) b = fma((double)__ldg(P.delta_b + (size_t)c * hr + j), hh[j], b);
-            a -= b;
-        } else if (c == 0) {
-            a = 0.28209479177387814;  // 1 / (2 sqrt(pi))
+#pragma unroll
+        for (int q = 0; q < 8; q++) {
+            const int v = v0 + lane + 32 * q;
+            if (v < V) odf[v] = (float)o[q];
         }
-        cf[c] = a;
-    }
-    __syncwarp();
-    for (int v = lane; v < V; v += kWarp) {
-        double o = 0.0;
-        for (int c = 0; c < C; c++) o = fma((double)__ldg(P.sampling + (size_t)v * C + c), cf[c], o);
-        odf[v] = (float)o;
     }
     __syncwarp();
 }
@@ -682,6 +759,7 @@ __global__ void __launch_bounds__(kBThreads, 1)
     rng.init(0, 0, 0);
     int rng_h = -1;
     unsigned long long rows_searched = 0, rows_refit = 0;  // lane-uniform per warp
+    const int nsl = batch_count(A.nsl_dev, A.nsl);
 
     for (;;) {
         // ---- refill empty slots from the queue of streamline halves
@@ -699,7 +777,7 @@ __global__ void __launch_bounds__(kBThreads, 1)
                 }
             } else if (my_h < 0 && !queue_empty) {
                 const int h = atomicAdd(A.hq, 1);
-                if (h >= 2 * A.nsl) {
+                if (h >= 2 * nsl) {
                     queue_empty = true;
                 } else {
                     my_h = h;
@@ -1097,8 +1175,8 @@ __global__ void __launch_bounds__(kBThreads, 1)
                     const int h = s_h[slot];
                     boot_refit_fp64(P, g.hr, g.HP / 16, A.volidx, s_pt[slot],
                                     A.nprobe > 0 ? A.probe_idx + (size_t)h * g.hr : nullptr,
-                                    A.rng_save + ((size_t)blockIdx.x * kSlots + slot) * 20,
-                                    A.refit_scr + ((size_t)blockIdx.x * kBWarps + w) * kRefitScr, odf_sh, lane);
+                                    A.rng_save + ((size_t)blockIdx.x * kSlots + slot) * 20, A.refit_tab,
+                                    A.refit_idx + ((size_t)blockIdx.x * kBWarps + w) * kRefitIdx, odf_sh, lane);
                     refitted = true;
                     rows_refit++;
                 }
@@ -1215,23 +1293,24 @@ cudaError_t launch_boot_batch_dwi(const float *src, const int *volidx, long long
 }
 
 cudaError_t launch_boot_batch_prep(const int *npeaks, const int *sl_off, const short *peaks, int max_store,
-                                   int n, int *sl_seed, short *sl_vert, int *status, cudaStream_t st) {
+                                   int n, int cap, int *sl_seed, short *sl_vert, int *status, cudaStream_t st) {
     const int grid = std::max(1, std::min((n + 255) / 256, 4096));
-    boot_batch_prep_kernel<<<grid, 256, 0, st>>>(npeaks, sl_off, peaks, max_store, n, sl_seed, sl_vert,
+    boot_batch_prep_kernel<<<grid, 256, 0, st>>>(npeaks, sl_off, peaks, max_store, n, cap, sl_seed, sl_vert,
                                                  status);
     return cudaGetLastError();
 }
 
-cudaError_t launch_boot_batch_join(const int *half_len, const int *sl_seed, int nsl, int *out_len,
-                                   int *out_seed, cudaStream_t st) {
+cudaError_t launch_boot_batch_join(const int *half_len, const int *sl_seed, int nsl, const int *count,
+                                   int *out_len, int *out_seed, cudaStream_t st) {
     const int grid = std::max(1, std::min((nsl + 255) / 256, 4096));
-    boot_batch_join_kernel<<<grid, 256, 0, st>>>(half_len, sl_seed, nsl, out_len, out_seed);
+    boot_batch_join_kernel<<<grid, 256, 0, st>>>(half_len, sl_seed, nsl, count, out_len, out_seed);
     return cudaGetLastError();
 }
 
 cudaError_t launch_gather_halves(const float *pool, const long long *half_off, const int *half_len,
-                                 const long long *pt_off, int nsl, float *out, int grid, cudaStream_t st) {
-    gather_halves_kernel<<<grid, 256, 0, st>>>(pool, half_off, half_len, pt_off, nsl, out);
+                                 const long long *pt_off, int nsl, const int *count, const int *status,
+                                 float *out, int grid, cudaStream_t st) {
+    gather_halves_kernel<<<grid, 256, 0, st>>>(pool, half_off, half_len, pt_off, nsl, count, status, out);
     return cudaGetLastError();
 }
 

@@ -90,7 +90,8 @@ struct csl_tracker {
     DevBuf<long long> bb_half_off;
     DevBuf<float> bb_odf, bb_pts, bb_dwi;
     DevBuf<uint32_t> bb_rng_save;                 // near-tie re-evaluation: saved Philox counters
-    DevBuf<double> bb_refit_scr;                  // float64 scratch, per warp
+    DevBuf<double> bb_refit_tab;                  // float64 transposed fit matrices (refit_tab_layout)
+    DevBuf<int> bb_refit_idx;                     // resample indices of a re-fit, per warp
     DevBuf<unsigned long long> bb_refit_count;    // rows searched, rows fitted again
     // compression of the last batch (csl_compress)
     DevBuf<float> cmp_world, cmp_pts;
@@ -265,7 +266,8 @@ static void release_all(csl_tracker *t) {
     t->bb_pts.release();
     t->bb_dwi.release();
     t->bb_rng_save.release();
-    t->bb_refit_scr.release();
+    t->bb_refit_tab.release();
+    t->bb_refit_idx.release();
     t->bb_refit_count.release();
     t->cmp_world.release();
     t->cmp_pts.release();
@@ -491,7 +493,27 @@ int csl_create(const csl_params *params, const csl_inputs *inputs, int device, c
                 CK(t->bb_odf.ensure(slots * g.vstride));
                 CK(t->bb_pts.ensure(slots * (size_t)p.max_sline_len * 3));
                 CK(t->bb_rng_save.ensure(slots * 4 * 5));
-                CK(t->bb_refit_scr.ensure((size_t)t->nsm * 16 * kRefitScr));
+                CK(t->bb_refit_idx.ensure((size_t)t->nsm * 16 * kRefitIdx));
+                {
+                    // float64 copies of the fit matrices, transposed for the re-fit's coalesced reads
+                    const int C = p.delta_nr, V = p.samplm_nr;
+                    const RefitTab L = refit_tab_layout(hr, C, V);
+                    std::vector<double> tab(L.total, 0.0);
+                    for (int i = 0; i < hr; i++)
+                        for (int j = 0; j < hr; j++) {
+                            tab[L.rh + 2 * ((size_t)i * hr + j)] = inputs->R[(size_t)j * hr + i];
+                            tab[L.rh + 2 * ((size_t)i * hr + j) + 1] = inputs->H[(size_t)j * hr + i];
+                        }
+                    for (int j = 0; j < hr; j++)
+                        for (int c = 0; c < C; c++) {
+                            tab[L.dq + (size_t)j * kRefitCP + c] = inputs->delta_q[(size_t)c * hr + j];
+                            tab[L.db + (size_t)j * kRefitCP + c] = inputs->delta_b[(size_t)c * hr + j];
+                        }
+                    for (int c = 0; c < C; c++)
+                        for (int v = 0; v < V; v++)
+                            tab[L.smp + (size_t)c * L.vp + v] = inputs->sampling_matrix[(size_t)v * C + c];
+                    if ((r = upload(t, t->bb_refit_tab, tab.data(), tab.size()))) return r;
+                }
                 CK(t->bb_refit_count.ensure(2));
                 CK(cudaMemsetAsync(t->bb_refit_count.p, 0, 2 * sizeof(unsigned long long), t->own_stream));
             }
@@ -585,15 +607,51 @@ int csl_destroy(csl_tracker *t) {
 // (the per-warp path recomputes them).
 static constexpr int kUsePerWarpPath = 1;
 
+// pass 2 of this tracker runs the batched tensor-core fit (whenever pass 1
+// stored every seed's initial directions)
+static bool uses_batched_fit(const csl_tracker *t) {
+    return t->hp.boot_fit >= 1 && (t->P.model == CSA || t->P.model == OPDT);
+}
+
 // Near-tie re-evaluation of the batched fit: on for boot_fit = 1, off for 2.
-// The flag margin is 2e-4 of the row maximum, 7x the largest BF16x3 ODF error
-// measured against float64 (2.9e-5).
+// The flag margin is 8e-5 of the row maximum: a decision compares two ODF
+// values, each off by at most 2.9e-5 of the row maximum in BF16x3 (the
+// largest error measured against float64), so only a gap below 5.8e-5 can
+// flip.
 static void set_refit(csl_tracker *t, BootBatchArgs &A) {
     A.refit = t->hp.boot_fit == 1 ? 1 : 0;
-    A.refit_tol = 2e-4f;
+    A.refit_tol = 8e-5f;
     A.rng_save = t->bb_rng_save.p;
-    A.refit_scr = t->bb_refit_scr.p;
+    A.refit_tab = t->bb_refit_tab.p;
+    A.refit_idx = t->bb_refit_idx.p;
     A.refit_count = t->bb_refit_count.p;
+}
+
+// the batched pass 2 of a batch of nsl streamlines (nsl: the slot capacity
+// when the count is read on the device), pool_cap points of pool
+static void boot_args(csl_tracker *t, BootBatchArgs &A, const float *seeds_dev, int nsl, long long rng_base,
+                      unsigned long long pool_cap) {
+    A.B1g = t->bb_B1.p;
+    A.B2g = t->bb_B2.p;
+    A.B3g = t->bb_B3.p;
+    A.volidx = t->bb_volidx.p;
+    A.nbr = t->bb_nbr.p;
+    A.dwi = t->bb_dwi.p;
+    A.seeds = seeds_dev;
+    A.sl_seed = t->bb_sl_seed.p;
+    A.sl_vert = t->bb_sl_vert.p;
+    A.nsl = nsl;
+    A.rng_base = rng_base;
+    A.hq = t->bb_hq.p;
+    A.odf = t->bb_odf.p;
+    A.pts = t->bb_pts.p;
+    A.pool_count = t->pool_count.p;
+    A.pool = t->pool.p;
+    A.pool_cap = pool_cap;
+    A.half_len = t->bb_half_len.p;
+    A.half_off = t->bb_half_off.p;
+    A.status = t->status.p;
+    set_refit(t, A);
 }
 
 static int run_boot_batch(csl_tracker *t, const float *seeds_dev, int ni, int nsl, long long rng_base,
@@ -605,7 +663,7 @@ static int run_boot_batch(csl_tracker *t, const float *seeds_dev, int ni, int ns
     CK(t->bb_half_len.ensure((size_t)2 * nsl + 2));
     CK(t->bb_half_off.ensure((size_t)2 * nsl + 2));
     CK(cudaMemsetAsync(t->status.p, 0, sizeof(int), st));
-    CK(launch_boot_batch_prep(t->npeaks.p, t->sl_off.p, t->peaks.p, kMaxStoredPeaksPerSeed, ni,
+    CK(launch_boot_batch_prep(t->npeaks.p, t->sl_off.p, t->peaks.p, kMaxStoredPeaksPerSeed, ni, nsl,
                               t->bb_sl_seed.p, t->bb_sl_vert.p, t->status.p, st));
     CK(cudaMemcpyAsync(t->host_stage, t->status.p, sizeof(int), cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
@@ -615,27 +673,7 @@ static int run_boot_batch(csl_tracker *t, const float *seeds_dev, int ni, int ns
     for (int attempt = 0; attempt < 2; attempt++) {
         CK(t->pool.ensure(want * 3));
         BootBatchArgs A{};
-        A.B1g = t->bb_B1.p;
-        A.B2g = t->bb_B2.p;
-        A.B3g = t->bb_B3.p;
-        A.volidx = t->bb_volidx.p;
-        A.nbr = t->bb_nbr.p;
-        A.dwi = t->bb_dwi.p;
-        A.seeds = seeds_dev;
-        A.sl_seed = t->bb_sl_seed.p;
-        A.sl_vert = t->bb_sl_vert.p;
-        A.nsl = nsl;
-        A.rng_base = rng_base;
-        A.hq = t->bb_hq.p;
-        A.odf = t->bb_odf.p;
-        A.pts = t->bb_pts.p;
-        A.pool_count = t->pool_count.p;
-        A.pool = t->pool.p;
-        A.pool_cap = t->pool.cap / 3;
-        A.half_len = t->bb_half_len.p;
-        A.half_off = t->bb_half_off.p;
-        A.status = t->status.p;
-        set_refit(t, A);
+        boot_args(t, A, seeds_dev, nsl, rng_base, t->pool.cap / 3);
         CK(cudaMemsetAsync(t->bb_hq.p, 0, sizeof(int), st));
         CK(cudaMemsetAsync(t->status.p, 0, sizeof(int), st));
         CK(cudaMemsetAsync(t->pool_count.p, 0, sizeof(unsigned long long), st));
@@ -656,7 +694,7 @@ static int run_boot_batch(csl_tracker *t, const float *seeds_dev, int ni, int ns
     }
 
     // join the halves, scan the lengths, gather
-    CK(launch_boot_batch_join(t->bb_half_len.p, t->bb_sl_seed.p, nsl, t->out_len.p, t->out_seed.p, st));
+    CK(launch_boot_batch_join(t->bb_half_len.p, t->bb_sl_seed.p, nsl, nullptr, t->out_len.p, t->out_seed.p, st));
     CK(cudaMemsetAsync(t->out_len.p + nsl, 0, sizeof(int), st));
     size_t tmpb = 0;
     CK(scan_temp_bytes(nsl + 1, &tmpb));
@@ -671,8 +709,8 @@ static int run_boot_batch(csl_tracker *t, const float *seeds_dev, int ni, int ns
     t->npts = npts;
     CK(t->points.ensure((size_t)npts * 3 + 3));
     if (nsl > 0)
-        CK(launch_gather_halves(t->pool.p, t->bb_half_off.p, t->bb_half_len.p, t->pt_off.p, nsl,
-                                t->points.p, t->nsm * 8, st));
+        CK(launch_gather_halves(t->pool.p, t->bb_half_off.p, t->bb_half_len.p, t->pt_off.p, nsl, nullptr,
+                                nullptr, t->points.p, t->nsm * 8, st));
     CK(cudaEventRecord(t->ev[4], st));
     CK(cudaStreamSynchronize(st));
     CK(cudaEventElapsedTime(&t->ms[0], t->ev[0], t->ev[1]));
@@ -683,10 +721,7 @@ static int run_boot_batch(csl_tracker *t, const float *seeds_dev, int ni, int ns
     return CSL_OK;
 }
 
-// per_warp_fit: track boot_fit = 1 trackers with the per-warp FP32 fit (the
-// multi-subject graph's path, so an overflowed subject's re-run matches it)
-static int run_batch(csl_tracker *t, const float *seeds_dev, long long n, long long rng_base,
-                     cudaStream_t st, bool per_warp_fit = false) {
+static int run_batch(csl_tracker *t, const float *seeds_dev, long long n, long long rng_base, cudaStream_t st) {
     const DevParams &P = t->P;
     t->ok_batch = 0;
     t->cmp_npts = -1;
@@ -727,7 +762,7 @@ static int run_batch(csl_tracker *t, const float *seeds_dev, long long n, long l
     CK(t->out_src.ensure((size_t)nsl + 1));
     CK(t->pt_off.ensure((size_t)nsl + 1));
 
-    if (t->hp.boot_fit >= 1 && !per_warp_fit && (P.model == CSA || P.model == OPDT)) {
+    if (uses_batched_fit(t)) {
         const int r = run_boot_batch(t, seeds_dev, ni, nsl, rng_base, st);
         if (r != kUsePerWarpPath) return r;
     }
@@ -1268,6 +1303,7 @@ static std::vector<const void *> branch_fingerprint(const csl_tracker *u) {
     return {u->npeaks.p, u->sl_off.p, u->peaks.p, u->out_len.p, u->out_seed.p, u->out_src.p, u->pt_off.p,
             u->pool.p, u->points.p, u->scratch.p, u->queue.p, u->status.p, u->pool_count.p, u->sort_tmp.p,
             u->mkeys.p, u->mkeys_sorted.p, u->mvals.p, u->perm.p, u->blk_next.p, u->blk_end.p,
+            u->bb_sl_seed.p, u->bb_sl_vert.p, u->bb_half_len.p, u->bb_half_off.p,
             (const void *)(intptr_t)u->block, (const void *)(intptr_t)u->blocks_per_sm,
             (const void *)(intptr_t)u->hp.seed_order};
 }
@@ -1297,6 +1333,13 @@ static int multi_size(csl_multi *m, int i) {
     CK(u->pt_off.ensure((size_t)cap + 1));
     CK(u->pool.ensure((size_t)pc * 3));
     CK(u->points.ensure((size_t)pc * 3 + 3));
+    if (uses_batched_fit(u)) {
+        CK(u->bb_sl_seed.ensure((size_t)cap + 1));
+        CK(u->bb_sl_vert.ensure((size_t)cap + 1));
+        CK(u->bb_half_len.ensure((size_t)2 * cap + 2));
+        CK(u->bb_half_off.ensure((size_t)2 * cap + 2));
+        return CSL_OK;
+    }
     const int grid2 = branch_grid(u, ni);
     CK(u->scratch.ensure((size_t)grid2 * (u->block / kWarp) * scratch_floats_per_warp(u->P)));
     if (u->hp.seed_order == 1) {
@@ -1329,6 +1372,27 @@ static int multi_record(csl_multi *m, int i, cudaStream_t s, cudaEvent_t wait_fo
     CK(launch_seed_peaks(P, m->seeds[i], ni, m->rng_base[i], u->partner.p, u->npeaks.p, u->peaks.p,
                          kMaxStoredPeaksPerSeed, grid1, u->block, s));
     CK(exclusive_scan_i32(m->scan_tmp[i].p, m->scan_tmp[i].cap, u->npeaks.p, u->sl_off.p, ni + 1, s));
+    const int *count = u->sl_off.p + ni;
+    if (uses_batched_fit(u)) {
+        // the batched tensor-core fit, its streamline count read on the device
+        CK(cudaMemsetAsync(u->status.p, 0, sizeof(int), s));
+        CK(launch_boot_batch_prep(u->npeaks.p, u->sl_off.p, u->peaks.p, kMaxStoredPeaksPerSeed, ni, cap,
+                                  u->bb_sl_seed.p, u->bb_sl_vert.p, u->status.p, s));
+        BootBatchArgs A{};
+        boot_args(u, A, m->seeds[i], cap, m->rng_base[i], m->pool_cap[i]);
+        A.nsl_dev = count;
+        CK(cudaMemsetAsync(u->bb_hq.p, 0, sizeof(int), s));
+        CK(cudaMemsetAsync(u->pool_count.p, 0, sizeof(unsigned long long), s));
+        if (wait_for) CK(cudaStreamWaitEvent(s, wait_for, 0));
+        CK(launch_boot_batch(P, u->bgeom, A, u->partner.p, u->nsm, s));
+        CK(cudaEventRecord(m->tracked[i], s));
+        CK(launch_boot_batch_join(u->bb_half_len.p, u->bb_sl_seed.p, cap, count, u->out_len.p, u->out_seed.p, s));
+        CK(launch_counted_scan(u->out_len.p, count, cap, m->bsum[i].p, u->pt_off.p, s));
+        CK(launch_gather_halves(u->pool.p, u->bb_half_off.p, u->bb_half_len.p, u->pt_off.p, cap, count,
+                                u->status.p, u->points.p, u->nsm * 8, s));
+        CK(launch_batch_summary(count, cap, u->pt_off.p, u->status.p, u->pool_count.p, m->summary.p + 4 * i, s));
+        return CSL_OK;
+    }
     BatchArgs B{};
     B.seeds = m->seeds[i];
     B.nseeds = ni;
@@ -1355,7 +1419,6 @@ static int multi_record(csl_multi *m, int i, cudaStream_t s, cudaEvent_t wait_fo
     CK(launch_track(P, B, u->partner.p, u->npeaks.p, u->peaks.p, kMaxStoredPeaksPerSeed, u->sl_off.p,
                     u->out_len.p, u->out_seed.p, u->out_src.p, grid2, u->block, s));
     CK(cudaEventRecord(m->tracked[i], s));
-    const int *count = u->sl_off.p + ni;
     CK(launch_counted_scan(u->out_len.p, count, cap, m->bsum[i].p, u->pt_off.p, s));
     CK(launch_gather_counted(u->pool.p, u->out_src.p, u->out_len.p, u->pt_off.p, count, cap, u->status.p,
                              (long long)m->pool_cap[i], u->points.p, u->nsm * 8, s));
@@ -1561,8 +1624,12 @@ int csl_multi_wait(csl_multi *m, long long *n_streamlines, long long *n_points, 
         csl_tracker *u = m->sub[i];
         const long long *S = m->summary_h + 4 * i;
         int again = 0;
-        if (m->n[i] > 0 && (S[2] & (ST_POOL_OVERFLOW | ST_SLOT_OVERFLOW))) {
-            const int rc = run_batch(u, m->seeds[i], m->n[i], m->rng_base[i], u->own_stream, true);
+        // overflowed capacities, or (batched fit) a seed with more initial
+        // directions than pass 1 stores: re-run on the plain path, which sizes
+        // exactly and takes the per-warp fit for such a batch as csl_propagate does
+        const int rerun = ST_POOL_OVERFLOW | ST_SLOT_OVERFLOW | (uses_batched_fit(u) ? ST_PEAKS_OVERFLOW : 0);
+        if (m->n[i] > 0 && (S[2] & rerun)) {
+            const int rc = run_batch(u, m->seeds[i], m->n[i], m->rng_base[i], u->own_stream);
             if (rc != CSL_OK) return fail(nullptr, rc, "subject %d: %s", i, u->err.c_str());
             m->sl_cap[i] = (int)std::min<long long>(
                 std::max<long long>(m->sl_cap[i], u->nsl + u->nsl / 8 + 256), (long long)INT32_MAX - 1);

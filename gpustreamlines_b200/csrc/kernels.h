@@ -75,7 +75,8 @@ struct BootBatchArgs {
     const float *seeds;
     const int *sl_seed;        // streamline -> seed (batch-local)
     const short *sl_vert;      // streamline -> initial vertex
-    int nsl;
+    int nsl;                   // streamlines (graph-captured batches: the slot capacity)
+    const int *nsl_dev;        // NULL, or the streamline count in device memory (clamped to nsl)
     long long rng_base;
     int *hq;                   // atomic queue of streamline halves
     float *odf;                // [grid * 128][vstride] ODF rows
@@ -100,25 +101,48 @@ struct BootBatchArgs {
     int refit;
     float refit_tol;
     uint32_t *rng_save;                 // [grid * 128 * 4][5]: Philox counter and index at each attempt's draws
-    double *refit_scr;                  // [grid * 16 warps][kRefitScr] float64 scratch
+    const double *refit_tab;            // float64 matrices, refit_tab_layout
+    int *refit_idx;                     // [grid * 16 warps][kRefitIdx] resample indices of a re-fit
     unsigned long long *refit_count;    // [2]: rows searched, rows fitted again
     // probe mode with directions: the chosen step of each probe item
     const float *probe_dirs;            // [nprobe, 3] incoming directions (NULL: ODF rows only)
     float *probe_step;                  // [nprobe, 4]: direction, found + 2 * (row fitted again)
 };
-constexpr int kRefitScr = 2048;         // doubles of float64 scratch per warp
+constexpr int kRefitIdx = 160;          // ints of re-fit scratch per warp (hr <= 160)
+
+// float64 tables of the near-tie re-fit (offsets in doubles): rh = (R[j][i],
+// H[j][i]) pairs at [i][j], dq / db = Delta_q / Delta_b transposed [hr][64],
+// smp = the sampling matrix transposed [C][vp], vp = V rounded up to 32
+constexpr int kRefitCP = 64;
+struct RefitTab {
+    size_t rh, dq, db, smp, total;
+    int vp;
+};
+__host__ __device__ inline RefitTab refit_tab_layout(int hr, int C, int V) {
+    RefitTab L;
+    L.vp = (V + 31) / 32 * 32;
+    L.rh = 0;
+    L.dq = L.rh + 2 * (size_t)hr * hr;
+    L.db = L.dq + (size_t)hr * kRefitCP;
+    L.smp = L.db + (size_t)hr * kRefitCP;
+    L.total = L.smp + (size_t)C * L.vp;
+    return L;
+}
 
 BootBatchGeom boot_batch_geom(const DevParams &P, int hr, int nb0);
 cudaError_t launch_boot_batch_pack(const DevParams &P, const BootBatchGeom &g, void *B1g, void *B2g,
                                    void *B3g, cudaStream_t st);
 cudaError_t launch_boot_batch_dwi(const float *src, const int *volidx, long long nvox, int T, int TP,
                                   float *dst, cudaStream_t st);
+// count (may be NULL): the streamline count in device memory, clamped to nsl
+// (graph-captured batches); status (may be NULL): gather nothing on overflow
 cudaError_t launch_boot_batch_prep(const int *npeaks, const int *sl_off, const short *peaks, int max_store,
-                                   int n, int *sl_seed, short *sl_vert, int *status, cudaStream_t st);
-cudaError_t launch_boot_batch_join(const int *half_len, const int *sl_seed, int nsl, int *out_len,
-                                   int *out_seed, cudaStream_t st);
+                                   int n, int cap, int *sl_seed, short *sl_vert, int *status, cudaStream_t st);
+cudaError_t launch_boot_batch_join(const int *half_len, const int *sl_seed, int nsl, const int *count,
+                                   int *out_len, int *out_seed, cudaStream_t st);
 cudaError_t launch_gather_halves(const float *pool, const long long *half_off, const int *half_len,
-                                 const long long *pt_off, int nsl, float *out, int grid, cudaStream_t st);
+                                 const long long *pt_off, int nsl, const int *count, const int *status,
+                                 float *out, int grid, cudaStream_t st);
 cudaError_t boot_batch_set_smem(const BootBatchGeom &g);
 cudaError_t launch_boot_odf_plain(const DevParams &P, const float *pts, const int *idx, int n, float *odf,
                                   int vstride, cudaStream_t st);

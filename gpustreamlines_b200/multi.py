@@ -9,7 +9,7 @@ to fixed-size seed batches and runs all of them as branches of ONE captured
 CUDA graph (``csl_multi_*`` in the C library): the GPU interleaves the
 subjects' CTAs, and the host waits once.  Each subject's streamlines are
 identical to its tracker's own ``generate_streamlines`` on the same seeds
-(bootstrap trackers always use the per-warp fit here).
+(bootstrap trackers with the batched tensor-core fit run it in the graph too).
 
     with GPUTracker(...) as a, GPUTracker(...) as b:
         run = MultiSubjectRun([a, b], [seeds_a, seeds_b])

@@ -70,7 +70,7 @@ typedef struct csl_params {
                                      reference's arithmetic (results identical to it); 1 = batched
                                      fit on the tensor cores in BF16x3 with FP32 accumulation, 128
                                      streamline halves per CTA, rows whose peak decisions lie within
-                                     2e-4 of the row maximum of flipping fitted again in float64
+                                     8e-5 of the row maximum of flipping fitted again in float64
                                      (CSA or OPDT; no counterpart in the reference, whose getter is
                                      the per-warp one, boot.cu:393-608); 2 = as 1 without the
                                      float64 re-evaluation */
@@ -337,14 +337,15 @@ int csl_seeds_from_mask(const float *mask_dev, int X, int Y, int Z, float thresh
  * to their seed batches (device float32 [n_seeds[i], 3]; pointers and counts
  * fixed for the plan's life, contents may be rewritten between launches) and
  * runs every batch as one branch of ONE captured CUDA graph: per subject,
- * pass 1, pass 2 (the per-warp tracking path: a boot_fit = 1 tracker is
- * tracked with the per-warp FP32 fit, in the graph and in an overflow re-run
- * alike) and compaction into the tracker's own result buffers, with no host
- * round trip.  Streamlines are identical to csl_propagate_device's for
- * trackers with boot_fit = 0 (any getter and sampler), and to those of the
- * same tracker created with boot_fit = 0 otherwise.  Slot capacity comes from a pass-1 count at creation, pool
- * capacity from points_per_streamline (0: 128); a subject that overflows
- * either is re-run on the plain path inside csl_multi_wait (replayed[i] = 1)
+ * pass 1, pass 2 (the tracker's own pass 2: the per-warp path, or the
+ * batched tensor-core fit for a CSA / OPDT tracker with boot_fit >= 1, its
+ * streamline count read on the device) and compaction into the tracker's own
+ * result buffers, with no host round trip.  Streamlines are identical to
+ * csl_propagate_device's for every tracker.  Slot capacity comes from a
+ * pass-1 count at creation, pool capacity from points_per_streamline (0:
+ * 128); a subject that overflows either (or, batched fit, has a seed with
+ * more initial directions than pass 1 stores, which csl_propagate tracks on
+ * the per-warp path) is re-run on the plain path inside csl_multi_wait (replayed[i] = 1)
  * and its capacities grow for the next launch, which re-captures the graph
  * (it also re-captures when a tracker's buffers or launch shape changed).
  *   csl_multi_launch  one cudaGraphLaunch on stream (NULL: the plan's own)

@@ -5,7 +5,8 @@ Bars, all bit-exact:
   * every subject's streamline lengths, seed indices and float32 points from
     the one-graph launch equal its own csl_propagate batch on the same seeds
     (mixed getters: probabilistic with two parameter sets, bootstrap CSA and
-    OPDT, PTT; one empty subject);
+    OPDT with the per-warp FP32 fit and with the batched tensor-core fit, PTT;
+    one empty subject);
   * the same on a second launch of the same graph, after seeds are rewritten
     in place, and when a pool far too small forces the plain-path re-run and
     a re-capture with grown capacities;
@@ -22,8 +23,13 @@ from test_gpu_parity import _handle
 
 pytestmark = pytest.mark.gpu
 
-NAMES = ["prob_s", "csa_s", "ptt_s", "opdt_s", "prob_v", "prob_s"]
-COUNTS = [3000, 400, 300, 0, 1500, 700]
+NAMES = ["prob_s", "csa_s", "ptt_s", "opdt_s", "prob_v", "prob_s", "csa_s", "opdt_s"]
+COUNTS = [3000, 400, 300, 0, 1500, 700, 600, 500]
+KW = [{}, {}, {}, {}, {}, {}, {"boot_fit": 1}, {"boot_fit": 1}]
+
+
+def _handles():
+    return [_handle(n, **kw) for n, kw in zip(NAMES, KW)]
 
 
 def _dev(seeds):
@@ -65,7 +71,7 @@ def test_multi_subject_graph_matches_plain_batches():
 
     from gpustreamlines_b200 import _lib
 
-    handles = [_handle(n) for n in NAMES]
+    handles = _handles()
     try:
         seeds = _seeds(21)
         dev = [_dev(s) for s in seeds]
@@ -115,7 +121,7 @@ def test_multi_subject_pool_overflow_reruns_and_recaptures():
 
     from gpustreamlines_b200 import _lib
 
-    handles = [_handle(n) for n in NAMES]
+    handles = _handles()
     try:
         seeds = _seeds(31)
         dev = [_dev(s) for s in seeds]

@@ -5,7 +5,10 @@ restated in PttDirectionGetter.prepare_data_host with numpy and a KD-tree):
   * the tiled, clipped, masked, normalised texture data identical, bit for bit;
   * the 128^3 nearest-vertex LUT identical except at exact distance ties
     (|d1 - d2| <= 1e-12 between the two candidates), which must be fewer than
-    1 in 10,000 grid points;
+    1 in 10,000 grid points -- apart from antipodal pairs when the sphere is
+    symmetric: there a vertex and its antipode are always at the same
+    distance (+-v), the KD-tree over [v; -v] picks either copy and the GPU
+    the lower index, and both address the same direction;
   * with the sphere symmetric and with a float64 threshold as well;
   * tracking through the Tracker API on the GPU-prepared data equals tracking
     on the host-prepared data when the LUTs agree everywhere.
@@ -37,6 +40,8 @@ def _lut_ties_ok(lut_gpu, lut_host, verts, res, symm):
         da = np.minimum(da, ((g + a) ** 2).sum(1))
         db = np.minimum(db, ((g + b) ** 2).sum(1))
     assert np.all(np.abs(da - db) <= 1e-12), np.abs(da - db).max()
+    if symm:  # antipodal pairs are the same direction
+        return int((np.abs(a + b).max(axis=1) > 1e-6).sum())
     return len(bad)
 
 
