@@ -513,33 +513,35 @@ __device__ __forceinline__ bool near_tie(const DevParams &P, const float *odf, c
 // h + r[idx], clamp at min_signal, division by the mean clamped b0 signal, the
 // CSA transform (coefficient 0 fixed) or the OPDT form, and the sphere
 // sampling; the row is rounded to float into odf.  Arithmetic of the float64
-// accuracy reference (oracle/fp64.py).
+// accuracy reference (oracle/fp64.py); the float32 matrix entries are exact in
+// double.
 //
-// Layout for speed: vectors over the hr non-b0 volumes live in registers,
-// element j in lane j % 32, slot j / 32 (hr <= 160), and are broadcast with
-// shuffles; the matrices come from the float64 tables of refit_tab_layout,
-// transposed so that a warp's 32 lanes read 32 consecutive entries.  idx:
-// hr ints of this warp's scratch.
+// Layout for speed (one warp, the tables in L2): vectors over the hr non-b0
+// volumes live in registers, element j in lane j % 32, slot j / 32
+// (hr <= 160), broadcast with shuffles; the tables of refit_tab_layout are
+// transposed so that the warp's 32 lanes read 32 consecutive entries, and the
+// loops are unrolled so that several rows of loads are in flight.  idx: hr
+// ints of this warp's scratch.
 constexpr int kRefitJ = 5;  // register slots per lane for an hr-vector (hr <= 160)
 
 __device__ __forceinline__ double shfl_d(double x, int src) { return __shfl_sync(FULL, x, src); }
 
-// element i of a register-distributed hr-vector (i warp-uniform)
-__device__ __forceinline__ double bcast(const double (&x)[kRefitJ], int i) {
+// slot k of a register-distributed hr-vector (k warp-uniform)
+__device__ __forceinline__ double slot_of(const double (&x)[kRefitJ], int k) {
     double r = 0.0;
 #pragma unroll
-    for (int k = 0; k < kRefitJ; k++)
-        if ((i >> 5) == k) r = x[k];
-    return shfl_d(r, i & 31);
+    for (int q = 0; q < kRefitJ; q++)
+        if (q == k) r = x[q];
+    return r;
 }
 
 __device__ __noinline__ void boot_refit_fp64(const DevParams &P, int hr, int nblk1, const int *__restrict__ volidx,
                                              float4 pt4, const int *pidx, const uint32_t *saved,
-                                             const double *__restrict__ tab, int *idx, float *odf, int lane) {
+                                             const float *__restrict__ tab, int *idx, float *odf, int lane) {
     const int T = P.dimt, C = P.delta_nr, V = P.samplm_nr;
     const RefitTab L = refit_tab_layout(hr, C, V);
-    const double2 *rh = reinterpret_cast<const double2 *>(tab + L.rh);
-    const double *dq = tab + L.dq, *db = tab + L.db, *smp = tab + L.smp;
+    const float2 *rh = reinterpret_cast<const float2 *>(tab + L.rh);
+    const float *dq = tab + L.dq, *db = tab + L.db, *smp = tab + L.smp;
     const double px = pt4.x, py = pt4.y, pz = pt4.z;
     const bool inb = (px >= -0.5) && (px + 0.5 < P.dimx) && (py >= -0.5) && (py + 0.5 < P.dimy) &&
                      (pz >= -0.5) && (pz + 0.5 < P.dimz);
@@ -599,22 +601,19 @@ __device__ __noinline__ void boot_refit_fp64(const DevParams &P, int hr, int nbl
 #pragma unroll
     for (int k = 0; k < kRefitJ; k++) rr[k] = hh[k] = 0.0;
     for (int i0 = 0; i0 < hr; i0 += 32) {
+        const double sc = slot_of(sv, i0 >> 5);
+        const int nb = min(32, hr - i0);
 #pragma unroll 4
-        for (int ii = 0; ii < 32; ii++) {
-            const int i = i0 + ii;
-            if (i >= hr) break;
-            double si = 0.0;
-#pragma unroll
-            for (int k = 0; k < kRefitJ; k++)
-                if ((i0 >> 5) == k) si = sv[k];
-            si = shfl_d(si, ii);
+        for (int ii = 0; ii < nb; ii++) {
+            const double si = shfl_d(sc, ii);
+            const float2 *row = rh + (size_t)(i0 + ii) * hr;
 #pragma unroll
             for (int k = 0; k < kRefitJ; k++) {
                 const int j = lane + 32 * k;
                 if (j < hr) {
-                    const double2 m = __ldg(rh + (size_t)i * hr + j);
-                    rr[k] = fma(m.x, si, rr[k]);
-                    hh[k] = fma(m.y, si, hh[k]);
+                    const float2 m = __ldg(row + j);
+                    rr[k] = fma((double)m.x, si, rr[k]);
+                    hh[k] = fma((double)m.y, si, hh[k]);
                 }
             }
         }
@@ -646,38 +645,44 @@ __device__ __noinline__ void boot_refit_fp64(const DevParams &P, int hr, int nbl
         }
         if (j >= hr) yv[k] = tv[k] = 0.0;
     }
-    // SH coefficients: lane c accumulates c and c + 32 over j in order
-    double cf[2] = {0.0, 0.0}, cb[2] = {0.0, 0.0};
-    for (int j = 0; j < hr; j++) {
-        const double tj = bcast(tv, j);
-        const double yj = opdt ? bcast(yv, j) : 0.0;
-#pragma unroll
-        for (int k = 0; k < 2; k++) {
-            const int c = lane + 32 * k;
-            if (c < C) {
-                cf[k] = fma(__ldg(dq + (size_t)j * kRefitCP + c), tj, cf[k]);
-                if (opdt) cb[k] = fma(__ldg(db + (size_t)j * kRefitCP + c), yj, cb[k]);
+    // SH coefficients: lane c accumulates c and c + 32 over j in order (the
+    // tables are zero past C)
+    double cf0 = 0.0, cf1 = 0.0, cb0 = 0.0, cb1 = 0.0;
+    for (int j0 = 0; j0 < hr; j0 += 32) {
+        const double tc = slot_of(tv, j0 >> 5), yc = slot_of(yv, j0 >> 5);
+        const int nb = min(32, hr - j0);
+#pragma unroll 8
+        for (int jj = 0; jj < nb; jj++) {
+            const double tj = shfl_d(tc, jj);
+            const float *dr = dq + (size_t)(j0 + jj) * kRefitCP;
+            cf0 = fma((double)__ldg(dr + lane), tj, cf0);
+            cf1 = fma((double)__ldg(dr + 32 + lane), tj, cf1);
+            if (opdt) {
+                const double yj = shfl_d(yc, jj);
+                const float *br = db + (size_t)(j0 + jj) * kRefitCP;
+                cb0 = fma((double)__ldg(br + lane), yj, cb0);
+                cb1 = fma((double)__ldg(br + 32 + lane), yj, cb1);
             }
         }
     }
-#pragma unroll
-    for (int k = 0; k < 2; k++) {
-        const int c = lane + 32 * k;
-        if (opdt) cf[k] -= cb[k];
-        else if (c == 0) cf[k] = 0.28209479177387814;  // 1 / (2 sqrt(pi))
+    if (opdt) {
+        cf0 -= cb0;
+        cf1 -= cb1;
+    } else if (lane == 0) {
+        cf0 = 0.28209479177387814;  // 1 / (2 sqrt(pi))
     }
     // sphere sampling: lane v accumulates vertices v + 32q over c in order, 8 at a time
     for (int v0 = 0; v0 < V; v0 += 8 * kWarp) {
         double o[8];
 #pragma unroll
         for (int q = 0; q < 8; q++) o[q] = 0.0;
+#pragma unroll 3
         for (int c = 0; c < C; c++) {
-            const double cc = shfl_d(c < 32 ? cf[0] : cf[1], c & 31);
+            const double cc = shfl_d(c < 32 ? cf0 : cf1, c & 31);
+            const float *sr = smp + (size_t)c * L.vp + v0 + lane;
 #pragma unroll
-            for (int q = 0; q < 8; q++) {
-                const int v = v0 + lane + 32 * q;
-                if (v < V) o[q] = fma(__ldg(smp + (size_t)c * L.vp + v), cc, o[q]);
-            }
+            for (int q = 0; q < 8; q++)
+                if (v0 + lane + 32 * q < L.vp) o[q] = fma((double)__ldg(sr + 32 * q), cc, o[q]);
         }
 #pragma unroll
         for (int q = 0; q < 8; q++) {
@@ -1315,11 +1320,13 @@ cudaError_t launch_gather_halves(const float *pool, const long long *half_off, c
 }
 
 cudaError_t boot_batch_set_smem(const BootBatchGeom &g) {
-    return cudaFuncSetAttribute(boot_batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, g.smem);
+    return raise_smem_limit(boot_batch_kernel, g.smem);
 }
 
 cudaError_t launch_boot_batch(const DevParams &P, const BootBatchGeom &g, const BootBatchArgs &A,
                               const int *partner, int grid, cudaStream_t st) {
+    const cudaError_t e = raise_smem_limit(boot_batch_kernel, g.smem);
+    if (e != cudaSuccess) return e;
     boot_batch_kernel<<<grid, kBThreads, g.smem, st>>>(P, g, A, partner);
     return cudaGetLastError();
 }

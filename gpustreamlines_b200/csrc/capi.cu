@@ -90,7 +90,7 @@ struct csl_tracker {
     DevBuf<long long> bb_half_off;
     DevBuf<float> bb_odf, bb_pts, bb_dwi;
     DevBuf<uint32_t> bb_rng_save;                 // near-tie re-evaluation: saved Philox counters
-    DevBuf<double> bb_refit_tab;                  // float64 transposed fit matrices (refit_tab_layout)
+    DevBuf<float> bb_refit_tab;                   // transposed fit matrices for the re-fit (refit_tab_layout)
     DevBuf<int> bb_refit_idx;                     // resample indices of a re-fit, per warp
     DevBuf<unsigned long long> bb_refit_count;    // rows searched, rows fitted again
     // compression of the last batch (csl_compress)
@@ -119,6 +119,7 @@ int tracker_view(csl_tracker *t, DevParams *P, const int **partner, int *device)
     return CSL_OK;
 }
 int tracker_fail(csl_tracker *t, int code, const char *msg) {
+    (void)cudaGetLastError();
     if (t)
         t->err = msg;
     else
@@ -128,6 +129,7 @@ int tracker_fail(csl_tracker *t, int code, const char *msg) {
 }  // namespace csl
 
 static int fail(csl_tracker *t, int code, const char *fmt, ...) {
+    (void)cudaGetLastError();  // a failed call's error must not surface in a later launch check
     char buf[512];
     va_list ap;
     va_start(ap, fmt);
@@ -495,10 +497,10 @@ int csl_create(const csl_params *params, const csl_inputs *inputs, int device, c
                 CK(t->bb_rng_save.ensure(slots * 4 * 5));
                 CK(t->bb_refit_idx.ensure((size_t)t->nsm * 16 * kRefitIdx));
                 {
-                    // float64 copies of the fit matrices, transposed for the re-fit's coalesced reads
+                    // the fit matrices transposed for the re-fit's coalesced reads
                     const int C = p.delta_nr, V = p.samplm_nr;
                     const RefitTab L = refit_tab_layout(hr, C, V);
-                    std::vector<double> tab(L.total, 0.0);
+                    std::vector<float> tab(L.total, 0.0f);
                     for (int i = 0; i < hr; i++)
                         for (int j = 0; j < hr; j++) {
                             tab[L.rh + 2 * ((size_t)i * hr + j)] = inputs->R[(size_t)j * hr + i];

@@ -150,7 +150,7 @@ cudaError_t launch_env_tables(const DevParams &P, const short *member, uint32_t 
 
 template <typename K>
 static cudaError_t set_smem_env(K kernel, int bytes) {
-    return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    return raise_smem_limit(kernel, bytes);
 }
 
 cudaError_t track_occupancy_env(const DevParams &P, int block, int *blocks_per_sm) {

@@ -275,7 +275,7 @@ __global__ void boot_odf_plain_kernel(DevParams P, const float *pts, const int *
 
 template <typename K>
 static cudaError_t set_smem(K kernel, int bytes) {
-    return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    return raise_smem_limit(kernel, bytes);
 }
 
 cudaError_t launch_seed_peaks(const DevParams &P, const float *seeds, int n, long long rng_base,

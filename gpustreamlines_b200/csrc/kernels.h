@@ -19,6 +19,19 @@ __host__ __device__ inline size_t scratch_floats_per_warp(const DevParams &P) {
 
 int smem_bytes(const DevParams &P, int warps, bool track);
 
+// Raise (never lower) a kernel's dynamic shared-memory limit.  Several
+// trackers launch the same kernel with their own sizes, and a captured graph
+// holds launches of several of them, so the limit only ever grows.
+template <typename K>
+inline cudaError_t raise_smem_limit(K kernel, int bytes) {
+    cudaFuncAttributes fa;
+    cudaError_t e = cudaFuncGetAttributes(&fa, reinterpret_cast<const void *>(kernel));
+    if (e != cudaSuccess) return e;
+    if (fa.maxDynamicSharedSizeBytes >= bytes) return cudaSuccess;
+    return cudaFuncSetAttribute(reinterpret_cast<const void *>(kernel), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                bytes);
+}
+
 cudaError_t launch_seed_peaks(const DevParams &P, const float *seeds, int n, long long rng_base,
                               const int *partner, int *npeaks, short *peaks, int max_store,
                               int grid, int block, cudaStream_t st);
@@ -101,7 +114,7 @@ struct BootBatchArgs {
     int refit;
     float refit_tol;
     uint32_t *rng_save;                 // [grid * 128 * 4][5]: Philox counter and index at each attempt's draws
-    const double *refit_tab;            // float64 matrices, refit_tab_layout
+    const float *refit_tab;             // transposed fit matrices, refit_tab_layout
     int *refit_idx;                     // [grid * 16 warps][kRefitIdx] resample indices of a re-fit
     unsigned long long *refit_count;    // [2]: rows searched, rows fitted again
     // probe mode with directions: the chosen step of each probe item
@@ -110,9 +123,10 @@ struct BootBatchArgs {
 };
 constexpr int kRefitIdx = 160;          // ints of re-fit scratch per warp (hr <= 160)
 
-// float64 tables of the near-tie re-fit (offsets in doubles): rh = (R[j][i],
-// H[j][i]) pairs at [i][j], dq / db = Delta_q / Delta_b transposed [hr][64],
-// smp = the sampling matrix transposed [C][vp], vp = V rounded up to 32
+// tables of the near-tie re-fit (float32 entries, exact in double; offsets in
+// floats): rh = (R[j][i], H[j][i]) pairs at [i][j], dq / db = Delta_q /
+// Delta_b transposed [hr][64], smp = the sampling matrix transposed [C][vp],
+// vp = V rounded up to 32; zero past C and V
 constexpr int kRefitCP = 64;
 struct RefitTab {
     size_t rh, dq, db, smp, total;

@@ -129,7 +129,10 @@ def gradient_table(bvals, bvecs, b0_threshold=50.0):
 
 def _dwi_design(gtab, sh_order_max, full_basis=False):
     b0s = np.asarray(gtab.b0s_mask, dtype=bool)
-    grads = np.asarray(gtab.gradients, dtype=np.float64)[~b0s]
+    grads = getattr(gtab, "gradients", None)
+    if grads is None:  # a duck-typed table with bvals / bvecs only (DIPY: gradients = bvals * bvecs)
+        grads = np.asarray(gtab.bvals, dtype=np.float64)[:, None] * np.asarray(gtab.bvecs, dtype=np.float64)
+    grads = np.asarray(grads, dtype=np.float64)[~b0s]
     _, theta, phi = cart2sphere(grads[:, 0], grads[:, 1], grads[:, 2])
     B, m_values, l_values = real_sh_descoteaux(sh_order_max, theta, phi, full_basis, legacy=True)
     return B, m_values, l_values
