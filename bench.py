@@ -202,7 +202,7 @@ def run_boot_compare(args):
     ph, sph, data, seeds = build_workload(0, args.seeds, "csa_bf16x3")
     d = _lib.DeviceBuffer.from_array(seeds, 0)
     out = {}
-    for fit in ("bf16x3", "bf16x3_nofp64", "fp32"):
+    for fit in ("bf16x3", "bf16x3_fp64", "fp32"):
         dg = BootDirectionGetter.from_dipy_csa(ph.gtab, sph, sh_order_max=8, fit=fit)
         with Tracker(dg, data, ph.fa, 0.1, sph.vertices, sph.edges, max_angle=math.radians(60), step_size=0.5) as tr:
             h = tr.handles[0]
@@ -240,7 +240,7 @@ def run_boot_compare(args):
                                         "peak_source": "measured MEASURED_PEAKS bf16_tflops"}
     print(json.dumps({"workload": f"bootstrap CSA getter, sh_order 8 (45 coeffs), 81x106x76x160 DWI, {args.seeds} seeds, "
                                   "step 0.5, max angle 60", "batched_bf16x3": out["bf16x3"],
-                      "batched_bf16x3_without_fp64_refit": out["bf16x3_nofp64"], "per_warp_fp32": out["fp32"],
+                      "batched_bf16x3_fp64_refit": out["bf16x3_fp64"], "per_warp_fp32": out["fp32"],
                       "speedup_bf16x3_vs_fp32": out["bf16x3"]["steps_per_s"] / out["fp32"]["steps_per_s"]}),
           flush=True)
     return 0

@@ -81,7 +81,7 @@ struct csl_tracker {
     DevBuf<unsigned char> scan_tmp, sort_tmp;
     DevBuf<uint32_t> mkeys, mkeys_sorted;
     DevBuf<int> mvals, perm, blk_next, blk_end;
-    // batched bootstrap fit (boot_fit == 1)
+    // batched bootstrap fit (boot_fit 1 or 2)
     BootBatchGeom bgeom{};
     DevBuf<unsigned char> bb_B1, bb_B2, bb_B3;
     DevBuf<int> bb_volidx, bb_sl_seed, bb_half_len, bb_hq;
@@ -317,9 +317,9 @@ static int validate(const csl_params *p, const csl_inputs *in, csl_tracker *t) {
                         p->samplm_nr, p->nvertices);
         if (p->boot_fit < 0 || p->boot_fit > 2) return fail(t, CSL_E_INVALID, "boot_fit must be 0, 1 or 2");
         if (p->boot_fit >= 1) {
-            if (p->dimt > 512) return fail(t, CSL_E_INVALID, "boot_fit=1 supports at most 512 volumes");
-            if (p->delta_nr > 64) return fail(t, CSL_E_INVALID, "boot_fit=1 supports at most 64 SH coefficients");
-            if (p->samplm_nr > 768) return fail(t, CSL_E_INVALID, "boot_fit=1 supports at most 768 sphere samples");
+            if (p->dimt > 512) return fail(t, CSL_E_INVALID, "the batched fit supports at most 512 volumes");
+            if (p->delta_nr > 64) return fail(t, CSL_E_INVALID, "the batched fit supports at most 64 SH coefficients");
+            if (p->samplm_nr > 768) return fail(t, CSL_E_INVALID, "the batched fit supports at most 768 sphere samples");
         }
     } else {
         if (p->nvertices != p->dimt)
@@ -448,7 +448,7 @@ int csl_create(const csl_params *params, const csl_inputs *inputs, int device, c
             P.b0s_mask = t->b0s.p;
             if (p.boot_fit >= 1) {
                 if (hr > 160)
-                    return fail(t, CSL_E_INVALID, "boot_fit=1 supports at most 160 non-b0 volumes, got %d", hr);
+                    return fail(t, CSL_E_INVALID, "the batched fit supports at most 160 non-b0 volumes, got %d", hr);
                 // volume order of the batched gather: non-b0 volumes, then b0s
                 std::vector<int> volidx;
                 for (int i = 0; i < p.dimt; i++)
@@ -470,7 +470,7 @@ int csl_create(const csl_params *params, const csl_inputs *inputs, int device, c
                         for (int d = 0; d < deg[q[0]]; d++) seen |= nbr[(size_t)q[0] * kMaxDegree + d] == q[1];
                         if (seen) continue;
                         if (deg[q[0]] == kMaxDegree)
-                            return fail(t, CSL_E_INVALID, "boot_fit=1 supports spheres of vertex degree <= %d",
+                            return fail(t, CSL_E_INVALID, "the batched fit supports spheres of vertex degree <= %d",
                                         kMaxDegree);
                         nbr[(size_t)q[0] * kMaxDegree + deg[q[0]]++] = (short)q[1];
                     }
@@ -478,7 +478,7 @@ int csl_create(const csl_params *params, const csl_inputs *inputs, int device, c
                 const BootBatchGeom g = boot_batch_geom(P, hr, p.dimt - hr);
                 t->bgeom = g;
                 if (g.smem > 227 * 1024)
-                    return fail(t, CSL_E_INVALID, "boot_fit=1 needs %d B of shared memory per block", g.smem);
+                    return fail(t, CSL_E_INVALID, "the batched fit needs %d B of shared memory per block", g.smem);
                 if ((r = upload(t, t->bb_volidx, volidx.data(), volidx.size()))) return r;
                 CK(t->bb_dwi.ensure(nvox * (size_t)g.TP));
                 CK(launch_boot_batch_dwi(t->dataf.p, t->bb_volidx.p, (long long)nvox, p.dimt, g.TP,
@@ -603,7 +603,7 @@ int csl_destroy(csl_tracker *t) {
     return CSL_OK;
 }
 
-// Pass 2 with the batched tensor-core fit (boot_fit == 1): streamline halves
+// Pass 2 with the batched tensor-core fit (boot_fit 1 or 2): streamline halves
 // are tracked independently, 128 per CTA, and joined afterwards.  Returns
 // kUsePerWarpPath when a seed has more initial directions than pass 1 stores
 // (the per-warp path recomputes them).
@@ -615,13 +615,13 @@ static bool uses_batched_fit(const csl_tracker *t) {
     return t->hp.boot_fit >= 1 && (t->P.model == CSA || t->P.model == OPDT);
 }
 
-// Near-tie re-evaluation of the batched fit: on for boot_fit = 1, off for 2.
+// Near-tie re-evaluation of the batched fit: on for boot_fit = 2, off for 1.
 // The flag margin is 8e-5 of the row maximum: a decision compares two ODF
 // values, each off by at most 2.9e-5 of the row maximum in BF16x3 (the
 // largest error measured against float64), so only a gap below 5.8e-5 can
 // flip.
 static void set_refit(csl_tracker *t, BootBatchArgs &A) {
-    A.refit = t->hp.boot_fit == 1 ? 1 : 0;
+    A.refit = t->hp.boot_fit == 2 ? 1 : 0;
     A.refit_tol = 8e-5f;
     A.rng_save = t->bb_rng_save.p;
     A.refit_tab = t->bb_refit_tab.p;
@@ -860,7 +860,7 @@ static int boot_probe(csl_tracker *t, const float *points_dev, const int *resamp
     if (n < 0 || n > (1ll << 30)) return fail(t, CSL_E_INVALID, "bad point count");
     if (fit != 0 && fit != 1) return fail(t, CSL_E_INVALID, "fit must be 0 or 1");
     if (fit == 1 && t->hp.boot_fit < 1)
-        return fail(t, CSL_E_STATE, "fit=1 needs a tracker created with boot_fit=1");
+        return fail(t, CSL_E_STATE, "fit=1 needs a tracker created with boot_fit 1 or 2");
     if (odf_stride < P.samplm_nr || odf_stride % 4 != 0)
         return fail(t, CSL_E_INVALID, "odf_stride must be >= samplm_nr and a multiple of 4");
     if (n == 0) return CSL_OK;

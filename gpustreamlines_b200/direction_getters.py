@@ -62,11 +62,11 @@ class BootDirectionGetter(GPUDirectionGetter):
         """``fit`` (keyword only, not in the reference): "fp32" runs the
         reference's per-warp FP32 fit with identical results; "bf16x3" runs the
         batched tensor-core fit (CSA or OPDT), 128 streamline halves per CTA with
-        BF16x3 products and FP32 accumulation, and fits again in float64 any row
-        whose peak decisions lie within the BF16x3 error of flipping;
-        "bf16x3_nofp64" is the batched fit without that re-evaluation."""
-        if fit not in ("fp32", "bf16x3", "bf16x3_nofp64"):
-            raise ValueError(f"Invalid fit {fit!r}, must be one of 'fp32', 'bf16x3', 'bf16x3_nofp64'")
+        BF16x3 products and FP32 accumulation; "bf16x3_fp64" is the batched fit
+        that also fits again in float64 any row whose peak decisions lie within
+        the BF16x3 error of flipping."""
+        if fit not in ("fp32", "bf16x3", "bf16x3_fp64"):
+            raise ValueError(f"Invalid fit {fit!r}, must be one of 'fp32', 'bf16x3', 'bf16x3_fp64'")
         self.fit = fit
         if model_type.upper() == "OPDT":
             self.model_type = _lib.MODEL_OPDT
@@ -107,7 +107,7 @@ class BootDirectionGetter(GPUDirectionGetter):
         if len(self.b0s_mask) != tracker.dimt:
             raise ValueError("b0s_mask length must match the last dimension of dataf")
         params.model = self.model_type
-        params.boot_fit = {"fp32": 0, "bf16x3": 1, "bf16x3_nofp64": 2}[self.fit]
+        params.boot_fit = {"fp32": 0, "bf16x3": 1, "bf16x3_fp64": 2}[self.fit]
         params.min_signal = float(self.min_signal)
         params.delta_nr = self.delta_nr
         params.samplm_nr = int(self.sampling_matrix.shape[0])

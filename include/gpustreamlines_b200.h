@@ -69,11 +69,11 @@ typedef struct csl_params {
     int boot_fit;                 /* bootstrap fit: 0 = one warp per streamline in FP32 with the
                                      reference's arithmetic (results identical to it); 1 = batched
                                      fit on the tensor cores in BF16x3 with FP32 accumulation, 128
-                                     streamline halves per CTA, rows whose peak decisions lie within
-                                     8e-5 of the row maximum of flipping fitted again in float64
-                                     (CSA or OPDT; no counterpart in the reference, whose getter is
-                                     the per-warp one, boot.cu:393-608); 2 = as 1 without the
-                                     float64 re-evaluation */
+                                     streamline halves per CTA (CSA or OPDT; no counterpart in the
+                                     reference, whose getter is the per-warp one, boot.cu:393-608);
+                                     2 = as 1, and rows whose peak decisions lie within 8e-5 of the
+                                     row maximum of flipping are fitted again in float64 before the
+                                     closest peak is chosen */
     /* PTT getter (PttDirectionGetter, cu_direction_getters.py:417-468) */
     int odf_lut_res;              /* nearest-vertex LUT resolution (128) */
     int step_frac;                /* STEP_FRAC = round(step / target_short_step) */
@@ -238,7 +238,7 @@ int csl_last_error(const csl_tracker *t, char *buf, int buflen);
  * of every non-b0 volume given (resample[n][hr], 0 <= index < hr) instead of
  * drawn, so that fits can be compared at a fixed state.  fit = 0: the
  * per-warp FP32 arithmetic of the tracking path; fit = 1: the batched
- * tensor-core BF16x3 fit (needs a tracker created with boot_fit = 1).  Row i
+ * tensor-core BF16x3 fit (needs a tracker created with boot_fit 1 or 2).  Row i
  * of odf (stride odf_stride >= samplm_nr, a multiple of 4) receives the
  * samplm_nr ODF values; points outside the data give a zero row.
  */
@@ -250,7 +250,7 @@ int csl_boot_odf(csl_tracker *tracker, const float *points_dev, const int *resam
  * counterpart in the reference): as csl_boot_odf with fit = 1, plus the peak
  * search and closest-peak choice for the incoming direction dirs_dev[i]
  * (float32 [n,3]), the near-tie float64 re-evaluation included when the
- * tracker has boot_fit = 1.  step_dev[i] (float32 [n,4]) = the new direction,
+ * tracker has boot_fit = 2.  step_dev[i] (float32 [n,4]) = the new direction,
  * and in .w: 1 if a peak was found, + 2 if the row was fitted again in float64.
  * csl_boot_refit_stats reads {rows searched, rows fitted again} of the batched
  * fit since creation or the last reset (reset != 0 zeroes them).
