@@ -152,14 +152,14 @@ __device__ __forceinline__ float avg_mask(int n, const int *__restrict__ mask, c
 }
 
 // closest_peak_d (boot.cu:115-193); peaks are vertices ind[0..npeaks)
-__device__ __forceinline__ int closest_peak(const DevParams &P, float3 direction, int npeaks,
+__device__ __forceinline__ int closest_peak(const DevParams &P, const float *verts, float3 direction, int npeaks,
                                             const int *ind, int lane, float3 *peak) {
     const float cos_similarity = P.cos_max_angle;
     float cpeak_dot = 0;
     int cpeak_idx = -1;
     for (int j = 0; j < npeaks; j += kWarp) {
         if (j + lane < npeaks) {
-            const float3 p = vert3(P.verts, ind[j + lane]);
+            const float3 p = vert3_any(verts, ind[j + lane]);
             const float dot = direction.x * p.x + direction.y * p.y + direction.z * p.z;
             if (fabsf(dot) > fabsf(cpeak_dot)) {
                 cpeak_dot = dot;
@@ -180,7 +180,7 @@ __device__ __forceinline__ int closest_peak(const DevParams &P, float3 direction
     cpeak_dot = __shfl_sync(FULL, cpeak_dot, 0);
     cpeak_idx = __shfl_sync(FULL, cpeak_idx, 0);
     if (cpeak_idx >= 0) {
-        const float3 p = vert3(P.verts, ind[cpeak_idx]);
+        const float3 p = vert3_any(verts, ind[cpeak_idx]);
         if (cpeak_dot >= cos_similarity) {
             *peak = p;
             return 1;
@@ -266,7 +266,7 @@ __device__ int boot_get_direction(const DevParams &P, Philox &rng, float3 dir, f
         if (NATTEMPTS == 1) return ndir;
         if (ndir > 0) {
             float3 peak;
-            const int found = closest_peak(P, dir, ndir, S.ind, lane, &peak);
+            const int found = closest_peak(P, P.verts, dir, ndir, S.ind, lane, &peak);
             __syncwarp();
             if (found) {
                 *newdir = peak;

@@ -75,6 +75,12 @@ BootBatchGeom boot_batch_geom(const DevParams &P, int hr, int nb0) {
     g.nbr_shorts = round_up(g.V * kMaxDegree, 8);
     g.smem = 1024 + g.r0 + g.r1 + g.r2 + 3 * kSlots * 16 + 2 * kSlots * 4 + g.nbr_shorts * 2 +
              kMaxSortLayers * kWarp * 4 + 128;
+    // the sphere vertices join shared memory when they fit in the per-CTA limit
+    g.verts_floats = round_up(3 * g.V, 4);
+    if (g.smem + g.verts_floats * 4 <= 227 * 1024)
+        g.smem += g.verts_floats * 4;
+    else
+        g.verts_floats = 0;
     return g;
 }
 
@@ -226,7 +232,7 @@ __device__ __forceinline__ void split8(const float (&x)[8], uint4 &hi, uint4 &lo
 
 // Tail of the peak search: kept maxima ind[0..n) in ascending vertex order ->
 // descending sort by value (the reference's network), minimum-separation filter.
-__device__ __forceinline__ int peaks_finish(const DevParams &P, const float *odf, int *ind, int n,
+__device__ __forceinline__ int peaks_finish(const DevParams &P, const float *vs, const float *odf, int *ind, int n,
                                             const int *partner_sh, int lane) {
     const unsigned lmask = (1u << lane) - 1u;
     if (n == 0) return 0;
@@ -240,7 +246,7 @@ __device__ __forceinline__ int peaks_finish(const DevParams &P, const float *odf
         warp_sort_desc(partner_sh, lane, k, v);
         // greedy minimum-separation filter: candidate i is kept unless a
         // kept peak before it lies within the separation angle
-        const float3 pv = vert3(P.verts, lane < n ? v : 0);
+        const float3 pv = vert3_any(vs, lane < n ? v : 0);
         unsigned kept = 1u;
         for (int i = 1; i < n; i++) {
             const float3 abc = make_float3(__shfl_sync(FULL, pv.x, i), __shfl_sync(FULL, pv.y, i),
@@ -260,10 +266,10 @@ __device__ __forceinline__ int peaks_finish(const DevParams &P, const float *odf
         int k = 1;
         for (int i = 1; i < n; i++) {
             const int vi = ind[i];
-            const float3 abc = vert3(P.verts, vi);
+            const float3 abc = vert3_any(vs, vi);
             int j = 0;
             for (; j < k; j++) {
-                const float3 d = vert3(P.verts, ind[j]);
+                const float3 d = vert3_any(vs, ind[j]);
                 float cs = abc.x * d.x + abc.y * d.y + abc.z * d.z;
                 if (P.sphere_symm) cs = fabsf(cs);
                 if (cs > P.cos_min_sep) break;
@@ -292,7 +298,7 @@ __device__ __forceinline__ int peaks_finish(const DevParams &P, const float *odf
 //  * the minimum-separation filter runs the reference's greedy loop with the
 //    inner scan over the kept peaks done by all lanes at once.
 // cand[] and ind[] may alias.  Returns the number of kept peaks, in ind[].
-__device__ __forceinline__ int peaks_sparse(const DevParams &P, float *odf, int *ind, int nr, float m,
+__device__ __forceinline__ int peaks_sparse(const DevParams &P, const float *vs, float *odf, int *ind, int nr, float m,
                                             const short *__restrict__ nbr, const int *partner_sh, int lane) {
     const unsigned lmask = (1u << lane) - 1u;
     const float thr = (float)(P.pmf_threshold * (double)m);
@@ -363,7 +369,7 @@ __device__ __forceinline__ int peaks_sparse(const DevParams &P, float *odf, int 
         n += __popc(msk);
     }
     __syncwarp();
-    return peaks_finish(P, odf, ind, n, partner_sh, lane);
+    return peaks_finish(P, vs, odf, ind, n, partner_sh, lane);
 }
 
 // Faster exact path of the same search.  A peak is kept only if
@@ -373,7 +379,7 @@ __device__ __forceinline__ int peaks_sparse(const DevParams &P, float *odf, int 
 // kept (often a minority of the 724), thresholded values computed on the fly.
 // Returns -1 (warp-uniform) when the arg-max is not a strict maximum or the
 // row maximum is not positive; the caller then runs peaks_sparse.
-__device__ __forceinline__ int peaks_fast(const DevParams &P, const float *odf, int *ind, int nr,
+__device__ __forceinline__ int peaks_fast(const DevParams &P, const float *vs, const float *odf, int *ind, int nr,
                                           const short *__restrict__ nbr, const int *partner_sh, int lane) {
     const unsigned lmask = (1u << lane) - 1u;
     float m = -FLT_MAX, mn = FLT_MAX;
@@ -411,34 +417,51 @@ __device__ __forceinline__ int peaks_fast(const DevParams &P, const float *odf, 
     }
     const float mm = m + (-odf_min);
     const float comp_thres = (float)(P.relative_peak_thresh * (double)mm);
-    int n = 0;
+    // vertices that could be kept (thresholded value - min >= comp_thres),
+    // compacted in ascending order into ind; then the local-maximum test on
+    // the compacted list with every lane busy, kept ones compacted in place
+    int nc = 0;
     for (int j = 0; j < nr; j += kWarp) {
         const int v = j + lane;
-        bool keep = false;
+        bool c = false;
         if (v < nr) {
             float x = odf[v];
             x = (x < thr) ? 0.0f : x;
-            if ((x - odf_min) >= comp_thres) {
-                const uint4 nb = *reinterpret_cast<const uint4 *>(nbr + v * kMaxDegree);
-                const uint32_t w4[4] = {nb.x, nb.y, nb.z, nb.w};
-                bool larger = false, smaller = false;
+            c = (x - odf_min) >= comp_thres;
+        }
+        const unsigned msk = __ballot_sync(FULL, c);
+        if (c) ind[nc + __popc(msk & lmask)] = v;
+        nc += __popc(msk);
+    }
+    __syncwarp();
+    int n = 0;
+    for (int c0 = 0; c0 < nc; c0 += kWarp) {
+        bool keep = false;
+        int v = 0;
+        if (c0 + lane < nc) {
+            v = ind[c0 + lane];
+            float x = odf[v];
+            x = (x < thr) ? 0.0f : x;
+            const uint4 nb = *reinterpret_cast<const uint4 *>(nbr + v * kMaxDegree);
+            const uint32_t w4[4] = {nb.x, nb.y, nb.z, nb.w};
+            bool larger = false, smaller = false;
 #pragma unroll
-                for (int q = 0; q < 4; q++) {
-                    float y0 = odf[w4[q] & 0xffffu], y1 = odf[w4[q] >> 16];
-                    y0 = (y0 < thr) ? 0.0f : y0;
-                    y1 = (y1 < thr) ? 0.0f : y1;
-                    larger |= (x < y0) | (x < y1);
-                    smaller |= (y0 < x) | (y1 < x);
-                }
-                keep = !larger && smaller;
+            for (int q = 0; q < 4; q++) {
+                float y0 = odf[w4[q] & 0xffffu], y1 = odf[w4[q] >> 16];
+                y0 = (y0 < thr) ? 0.0f : y0;
+                y1 = (y1 < thr) ? 0.0f : y1;
+                larger |= (x < y0) | (x < y1);
+                smaller |= (y0 < x) | (y1 < x);
             }
+            keep = !larger && smaller;
         }
         const unsigned msk = __ballot_sync(FULL, keep);
+        __syncwarp();  // every lane has read its entry before any is overwritten
         if (keep) ind[n + __popc(msk & lmask)] = v;
         n += __popc(msk);
     }
     __syncwarp();
-    return peaks_finish(P, odf, ind, n, partner_sh, lane);
+    return peaks_finish(P, vs, odf, ind, n, partner_sh, lane);
 }
 
 // ---------------------------------------------------------------------------
@@ -451,7 +474,8 @@ __device__ __forceinline__ int peaks_fast(const DevParams &P, const float *odf, 
 // which of the two the separation filter keeps).  The BF16x3 row differs from
 // the float64 one by ~3e-5 of its maximum at most, so a row without such a
 // decision selects the float64 row's peaks.
-__device__ __forceinline__ bool near_tie(const DevParams &P, const float *odf, const int *ind, int n, int nr,
+__device__ __forceinline__ bool near_tie(const DevParams &P, const float *vs, const float *odf, const int *ind, int n,
+                                         int nr,
                                          const short *__restrict__ nbr, float tol, int lane) {
     float m = -FLT_MAX;
     for (int v = lane; v < nr; v += kWarp) m = fmax_ref(m, odf[v]);
@@ -487,14 +511,14 @@ __device__ __forceinline__ bool near_tie(const DevParams &P, const float *odf, c
             hit = true;
             continue;
         }
-        const float3 pv = vert3(P.verts, v);
+        const float3 pv = vert3_any(vs, v);
         for (int k = 0; k < n; k++) {
             const int p = ind[k];
             if (p == v) continue;
             float y = odf[p];
             y = y < thr ? 0.0f : y;
             if (fabsf(y - x) > tm) continue;
-            const float3 pp = vert3(P.verts, p);
+            const float3 pp = vert3_any(vs, p);
             float cs = pv.x * pp.x + pv.y * pp.y + pv.z * pp.z;
             if (P.sphere_symm) cs = fabsf(cs);
             if (cs > P.cos_min_sep) {
@@ -721,12 +745,16 @@ __global__ void __launch_bounds__(kBThreads, 1)
     uint64_t *bars = reinterpret_cast<uint64_t *>(partner_sh + kMaxSortLayers * kWarp);
     // bars: 0, 1 = B1 stage loaded; 2, 3 = B1 stage consumed; 4 = MMA batch done; 5 = B2/B3 loaded
     uint32_t *tmem_sh = reinterpret_cast<uint32_t *>(bars + 6);
+    float *verts_smem = reinterpret_cast<float *>(tmem_sh + 4);  // [3 V] sphere vertices, when they fit
+    const float *verts_sh = g.verts_floats ? verts_smem : P.verts;
 
     const int t = threadIdx.x, w = t >> 5, lane = t & 31;
     const int qd = w & 3, part = w >> 2;        // epilogue: lane quadrant, column share
     const int eslot = qd * 32 + lane;           // epilogue slot of this thread
     for (int i = t; i < kMaxSortLayers * kWarp; i += kBThreads) partner_sh[i] = partner[i];
     for (int i = t; i < g.V * kMaxDegree; i += kBThreads) nbr_sh[i] = A.nbr[i];
+    if (g.verts_floats)
+        for (int i = t; i < 3 * g.V; i += kBThreads) verts_smem[i] = P.verts[i];
     if (t < kSlots) s_h[t] = -1;
     if (t == 0) {
         for (int b = 0; b < 6; b++) mbar_init(&bars[b], 1);
@@ -1166,16 +1194,16 @@ __global__ void __launch_bounds__(kBThreads, 1)
                 int ndir = -1;
                 bool refitted = false;
                 for (int pass = 0; pass < 2; pass++) {
-                    ndir = peaks_fast(P, odf_sh, ind_sh, g.V, nbr_sh, partner_sh, lane);
+                    ndir = peaks_fast(P, verts_sh, odf_sh, ind_sh, g.V, nbr_sh, partner_sh, lane);
                     if (ndir < 0) {
                         float m = -FLT_MAX;
                         for (int v = lane; v < g.V; v += kWarp) m = fmax_ref(m, odf_sh[v]);
                         m = warp_max_ref(m);
-                        ndir = peaks_sparse(P, odf_sh, ind_sh, g.V, m, nbr_sh, partner_sh, lane);
+                        ndir = peaks_sparse(P, verts_sh, odf_sh, ind_sh, g.V, m, nbr_sh, partner_sh, lane);
                     }
                     if (pass == 1 || !A.refit) break;
                     rows_searched++;
-                    if (!near_tie(P, odf_sh, ind_sh, ndir, g.V, nbr_sh, A.refit_tol, lane)) break;
+                    if (!near_tie(P, verts_sh, odf_sh, ind_sh, ndir, g.V, nbr_sh, A.refit_tol, lane)) break;
                     // the decision is within the BF16x3 error: fit this row again in float64
                     const int h = s_h[slot];
                     boot_refit_fp64(P, g.hr, g.HP / 16, A.volidx, s_pt[slot],
@@ -1189,7 +1217,7 @@ __global__ void __launch_bounds__(kBThreads, 1)
                 float3 pk = make_float3(0, 0, 0);
                 if (ndir > 0) {
                     const float4 d4 = s_dir[slot];
-                    found = closest_peak(P, make_float3(d4.x, d4.y, d4.z), ndir, ind_sh, lane, &pk);
+                    found = closest_peak(P, verts_sh, make_float3(d4.x, d4.y, d4.z), ndir, ind_sh, lane, &pk);
                 }
                 __syncwarp();
                 if (lane == 0) {

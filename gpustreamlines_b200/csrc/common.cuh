@@ -225,6 +225,10 @@ __device__ __forceinline__ void warp_sort_desc(const int *__restrict__ partner_s
 __device__ __forceinline__ float3 vert3(const float *__restrict__ verts, int i) {
     return make_float3(__ldg(verts + 3 * i), __ldg(verts + 3 * i + 1), __ldg(verts + 3 * i + 2));
 }
+// the same from global or shared memory (generic loads; __ldg is global-only)
+__device__ __forceinline__ float3 vert3_any(const float *verts, int i) {
+    return make_float3(verts[3 * i], verts[3 * i + 1], verts[3 * i + 2]);
+}
 
 // ---------------------------------------------------------------------------
 // peak extraction (tracking_helpers.cu:75-245): local maxima over sphere

@@ -76,6 +76,7 @@ struct BootBatchGeom {
     int b1_chunk, b2_bytes, b3_chunk;  // bytes of one packed operand chunk (hi + lo)
     int r0, r1, r2, smem;              // shared-memory regions and total
     int nbr_shorts;                    // V * kMaxDegree, padded to 16 bytes
+    int verts_floats;                  // 3 V sphere-vertex coordinates in shared memory, padded to 4
 };
 
 struct BootBatchArgs {
