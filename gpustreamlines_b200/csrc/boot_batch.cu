@@ -1088,6 +1088,13 @@ __global__ void __launch_bounds__(kBThreads, 1)
             tc_fence_after();
         }
 
+        // ---- the first B3 chunk streams into R1 (free: the second product has
+        //      completed) while epilogue 2 runs
+        if (t == 0 && ok) {
+            mbar_arrive_expect_tx(&bars[5], (uint32_t)g.b3_chunk);
+            bulk_g2s(R1, A.B3g, (uint32_t)g.b3_chunk, &bars[5]);
+        }
+
         // ---- epilogue 2: SH coefficients -> A3 (coefficient 0 fixed, boot.cu CSA branch)
         for (int b = part; b < g.N2 / 16; b += 4) {
             float v[16];
@@ -1116,9 +1123,7 @@ __global__ void __launch_bounds__(kBThreads, 1)
         if (A.nprobe > 0 && s_live[eslot]) e_odf = A.probe_odf + (size_t)s_h[eslot] * A.probe_stride;
         for (int ch = 0; ch < g.nchunk3; ch++) {
             if (t == 0 && ok) {
-                mbar_arrive_expect_tx(&bars[5], (uint32_t)g.b3_chunk);
-                bulk_g2s(R1, A.B3g + (size_t)ch * g.b3_chunk, (uint32_t)g.b3_chunk, &bars[5]);
-                ok = mbar_wait(&bars[5], ph_aux);
+                ok = mbar_wait(&bars[5], ph_aux);  // chunk ch (issued before epilogue 2 or the last epilogue)
                 ph_aux ^= 1;
                 if (ok) {
                     tc_fence_after();
@@ -1140,6 +1145,11 @@ __global__ void __launch_bounds__(kBThreads, 1)
             if (!mbar_wait(&bars[4], ph_mma)) ok = false;
             ph_mma ^= 1;
             tc_fence_after();
+            // the next chunk streams into R1 (this chunk's product has read it) during this epilogue
+            if (t == 0 && ok && ch + 1 < g.nchunk3) {
+                mbar_arrive_expect_tx(&bars[5], (uint32_t)g.b3_chunk);
+                bulk_g2s(R1, A.B3g + (size_t)(ch + 1) * g.b3_chunk, (uint32_t)g.b3_chunk, &bars[5]);
+            }
             for (int b = part; b < kOdfChunk / 16; b += 4) {
                 float v[16];
                 tmem_ld16(trow + 16 * b, v);
