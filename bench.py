@@ -66,6 +66,8 @@ def parse():
     ap.add_argument("--multi", action="store_true",
                     help="multi-subject run: uneven subjects, mixed getters, one CUDA-graph launch")
     ap.add_argument("--subjects", type=int, default=12)
+    ap.add_argument("--multi-boot-fit", choices=("fp32", "bf16x3"), default="fp32",
+                    help="bootstrap subjects of --multi: per-warp FP32 fit or the batched tensor-core fit")
     ap.add_argument("--autotune", action="store_true",
                     help="print the launch-shape tuner's timings on this workload's seeds and exit")
     ap.add_argument("--learned", action="store_true",
@@ -444,7 +446,7 @@ def run_odf_volume(args):
     return 0
 
 
-def multi_subjects(nsub: int, seed: int = 5):
+def multi_subjects(nsub: int, seed: int = 5, boot_fit: str = "fp32"):
     """Uneven synthetic subjects for the multi-subject run: volumes log-uniform
     between 48^3 and 96x116x96 voxels (phantom shape scaled), two diffusion
     schemes (6 b0 + 64 dirs at b=1000, 2.5 mm; 10 b0 + 150 dirs at b=2000,
@@ -452,9 +454,11 @@ def multi_subjects(nsub: int, seed: int = 5):
     for bootstrap and PTT subjects, whose steps cost 40-120x a probabilistic
     step), getters
     cycling probabilistic, bootstrap CSA, PTT, probabilistic, bootstrap OPDT,
-    probabilistic."""
+    probabilistic.  boot_fit "bf16x3" gives the bootstrap subjects the batched
+    tensor-core fit (same subjects and seeds)."""
     rng = np.random.default_rng(seed)
-    cycle = ["prob", "csa", "ptt", "prob", "opdt", "prob"]
+    b = "_bf16x3" if boot_fit == "bf16x3" else ""
+    cycle = ["prob", "csa" + b, "ptt", "prob", "opdt" + b, "prob"]
     vox = np.exp(rng.uniform(np.log(48 ** 3), np.log(96 * 116 * 96), nsub))
     nseeds = np.exp(rng.uniform(np.log(5_000), np.log(250_000), nsub)).astype(int)
     out = []
@@ -481,7 +485,7 @@ def run_multi(args):
     from gpustreamlines_b200.sphere import get_sphere
 
     sph = get_sphere("repulsion724")
-    subs = multi_subjects(args.subjects)
+    subs = multi_subjects(args.subjects, boot_fit=args.multi_boot_fit)
     trackers, seeds, vol_bytes = [], [], 0
     t_setup = time.perf_counter()
     for sd in subs:
