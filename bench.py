@@ -536,8 +536,15 @@ def run_multi(args):
     multi_ms, replays, graph_med = by_k[2]
     captures, _, _ = run.plan.info()
 
-    # the same batches one after another through the plain path
-    dev = [t for t, _ in run._seeds]
+    # the same batches one after another through the plain path (the plan's
+    # device seed buffers, viewed as tensors for the stream-ordered copies below)
+    def tensor_view(buf):
+        class _View:
+            __cuda_array_interface__ = {"shape": buf.shape, "typestr": "<f4", "data": (buf.ptr, False),
+                                        "version": 3, "strides": None}
+        return torch.as_tensor(_View(), device="cuda")
+
+    dev = [tensor_view(t) for t, _ in run._seeds]
     handles = [tr.handles[0] for tr in trackers]
     for h, d, s in zip(handles, dev, seeds):
         h.propagate_device(d.data_ptr(), len(s), 0, stream.cuda_stream)
@@ -590,7 +597,7 @@ def run_multi(args):
                    "graph_device_ms": graph_med, "graph_captures": captures,
                    "replays_in_timed_region": replays, "max_concurrent_tracking_kernels": 2,
                    "ms_per_step_by_max_concurrent": {str(k): v[0] for k, v in sorted(by_k.items())},
-                   "bootstrap_fit": "per-warp FP32 (the graph path)"},
+                   "bootstrap_fit": {"fp32": "per-warp FP32", "bf16x3": "batched tensor-core BF16x3"}[args.multi_boot_fit]},
         "sequential_plain": {"value": seq_steps / (seq_ms / 1e3), "ms_per_step": seq_ms,
                              "note": "same batches, one csl_propagate_device per subject in turn"},
         "speedup_vs_sequential": seq_ms / multi_ms,
