@@ -78,6 +78,7 @@ constexpr int kPttRounds = 1024 / kWarp;  // 1024 candidates at most per directi
 #define CSL_PTT_WAVE 2
 #endif
 constexpr int kProbeWave = CSL_PTT_WAVE;  // probe points whose fetches are issued together
+constexpr int kPttFirst = 8;              // candidates probed before the rest of a round
 constexpr float kCurvMin = 1e-4f;         // |k1|, |k2| below this count as straight / are raised to it
 constexpr float kTinyNorm2 = 1e-8f;
 
@@ -344,13 +345,24 @@ __device__ int ptt_step_direction(const DevParams &P, PhiloxN &rng, float3 dir, 
         const float kx = fmaf(r2, k2.x - k0.x, fmaf(r1, k1.x - k0.x, k0.x));
         const float ky = fmaf(r2, k2.y - k0.y, fmaf(r1, k1.y - k0.y, k0.y));
         Frame3 G = INIT ? random_frame(t0, rng) : load_frame(frame_sh);
-        const float s = arc_support(P, pos, G, make_arc(kx, ky, P.probe_step_size), base, nprobe);
+        const Arc arc = make_arc(kx, ky, P.probe_step_size);
         unsigned won;
         if (INIT) {
+            const float s = arc_support(P, pos, G, arc, base, nprobe);
             const float best = warp_max_ref(s);
             won = __ballot_sync(FULL, s == best && (double)best >= thr);
         } else {
-            won = __ballot_sync(FULL, (double)s >= thr);
+            // the lowest lane whose candidate has enough support wins: candidates
+            // 0..kPttFirst-1 are probed first, the others only when none of those
+            // passes (every lane has drawn its numbers, so the result and the
+            // streams are those of probing all 32 at once)
+            won = 0u;
+            for (int pass = 0; pass < 2 && won == 0u; pass++) {
+                const bool mine = (lane < kPttFirst) == (pass == 0);
+                float s = 0.0f;
+                if (mine) s = arc_support(P, pos, G, arc, base, nprobe);
+                won = __ballot_sync(FULL, mine && (double)s >= thr);
+            }
         }
         if (won == 0u) continue;
         const int src = __ffs(won) - 1;
