@@ -210,9 +210,8 @@ __device__ __forceinline__ int env_sample(const DevParams &P, const int (&vox)[8
         const int nk = __popc(mk);
         int r = (int)(b * (float)nk);
         if (r >= nk) r = nk - 1;
-        unsigned mm = mk;
-        for (int i = 0; i < r; i++) mm &= mm - 1u;
-        const int v = (nk > 0) ? (int)__ldg(P.env_member + k * kEnvMaxMembers + (__ffs(mm) - 1)) : -1;
+        const int pos = (nk > 0) ? (int)__fns(mk, 0u, r + 1) : 0;  // r-th set bit of mk (0-based r)
+        const int v = (nk > 0) ? (int)__ldg(P.env_member + k * kEnvMaxMembers + pos) : -1;
         // P(v): lane 8g+q reads corner q, the group combines in corner order
         float dv = 0.0f;
         if (v >= 0) dv = __ldg(P.dataf + (size_t)myvox * P.dimt + v);
