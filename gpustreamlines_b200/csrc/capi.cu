@@ -494,10 +494,11 @@ int csl_create(const csl_params *params, const csl_inputs *inputs, int device, c
                 const size_t slots = (size_t)t->nsm * 128;
                 CK(t->bb_odf.ensure(slots * g.vstride));
                 CK(t->bb_pts.ensure(slots * (size_t)p.max_sline_len * 3));
-                CK(t->bb_rng_save.ensure(slots * 4 * 5));
-                CK(t->bb_refit_idx.ensure((size_t)t->nsm * 16 * kRefitIdx));
-                {
-                    // the fit matrices transposed for the re-fit's coalesced reads
+                if (p.boot_fit == 2) {
+                    // the near-tie re-fit: saved Philox counters, per-warp index
+                    // scratch, and the fit matrices transposed for coalesced reads
+                    CK(t->bb_rng_save.ensure(slots * 4 * 5));
+                    CK(t->bb_refit_idx.ensure((size_t)t->nsm * 16 * kRefitIdx));
                     const int C = p.delta_nr, V = p.samplm_nr;
                     const RefitTab L = refit_tab_layout(hr, C, V);
                     std::vector<float> tab(L.total, 0.0f);
