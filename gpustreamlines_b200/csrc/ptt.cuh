@@ -78,7 +78,7 @@ constexpr int kPttRounds = 1024 / kWarp;  // 1024 candidates at most per directi
 #define CSL_PTT_WAVE 2
 #endif
 constexpr int kProbeWave = CSL_PTT_WAVE;  // probe points whose fetches are issued together
-constexpr int kPttFirst = 2;              // candidates probed before the rest of a round
+constexpr int kPttFirst = 1;              // candidates probed before the rest of a round
 constexpr float kCurvMin = 1e-4f;         // |k1|, |k2| below this count as straight / are raised to it
 constexpr float kTinyNorm2 = 1e-8f;
 
